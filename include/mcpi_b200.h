@@ -1,0 +1,131 @@
+/* mcpi_b200 -- native C ABI of the B200 multiconfigurational hot path.
+ *
+ * One "space" is the Fock space of N bosons in M orbitals (1 <= M <= 16,
+ * NC(N,M) = C(N+M-1,N) < 2^31) resident on one CUDA device. Every array
+ * argument named d_* is a device pointer; complex numbers are two doubles
+ * (re, im), layout-compatible with C99 `double complex`, std::complex<double>
+ * and cuDoubleComplex. Work is enqueued on the space's stream and is complete
+ * after mcpi_space_sync() (functions returning host results synchronise).
+ * Every function returns MCPI_OK or an error code; mcpi_last_error() gives a
+ * message for the calling thread. Nothing aborts the process.
+ *
+ * Reference counterparts (andriati-alex/mcpi, file:line) are named beside each
+ * entry point. The reference-named drop-in interface (NC, setupFocks,
+ * applyHconf_XX, OBrho_XM, TBrho_XX, ...) is declared in mcpi_dropin.h and
+ * implemented on top of this one.
+ */
+#ifndef MCPI_B200_H
+#define MCPI_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define MCPI_API __attribute__((visibility("default")))
+#else
+#define MCPI_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MCPI_OK 0
+#define MCPI_ERR_ARG 1          /* invalid argument (sizes, NULL pointers) */
+#define MCPI_ERR_RANGE 2        /* NC(N,M) or a table size exceeds the supported range */
+#define MCPI_ERR_CUDA 3         /* a CUDA runtime call failed */
+#define MCPI_ERR_NOMEM 4        /* device or host allocation failed */
+#define MCPI_ERR_STATE 5        /* call order (e.g. no integrals set) */
+#define MCPI_ERR_NUMERIC 6      /* tridiagonal eigensolver did not converge */
+
+/* variants of the two-body folding (see mcpi_set_integrals) */
+#define MCPI_VARIANT_MAPS 0     /* applyHconf_X / _XX / _omp and the CUDA kernel */
+#define MCPI_VARIANT_HASH 1     /* applyHconf (plain): Rule 9 summed over all orderings */
+
+typedef struct mcpi_space_s *mcpi_space;
+
+MCPI_API const char *mcpi_status_string(int status);
+MCPI_API const char *mcpi_last_error(void);
+
+/* NC(N,M) = C(N+M-1, N), exact (configurationsMap.h:145-202, NC). */
+MCPI_API int mcpi_nc(int N, int M, int64_t *nc);
+
+/* Create / destroy a space on `device` (configurationsMap.h:206-344 state:
+ * NCmat + IF tables; here only the binomial table W and sqrt table are kept). */
+MCPI_API int mcpi_space_create(int N, int M, int device, mcpi_space *out);
+MCPI_API int mcpi_space_destroy(mcpi_space sp);
+/* Enqueue all further work of the space on `stream` (a cudaStream_t; NULL is the
+ * legacy default stream). A new space uses a private non-blocking stream. */
+MCPI_API int mcpi_space_set_stream(mcpi_space sp, void *stream);
+MCPI_API int mcpi_space_sync(mcpi_space sp);
+MCPI_API int mcpi_space_dims(mcpi_space sp, int *N, int *M, int64_t *nc);
+
+/* ---- tables in the reference layouts, built on the device ---------------- */
+/* NCmat[n + (N+1)*m] = NC(n,m), host output (configurationsMap.h:206-234). */
+MCPI_API int mcpi_ncmat(int N, int M, int32_t *h_ncmat);
+/* index <-> occupations, host scalars (configurationsMap.h:238-305). */
+MCPI_API int mcpi_index_to_fock(int N, int M, int64_t index, int32_t *h_v);
+MCPI_API int mcpi_fock_to_index(int N, int M, const int32_t *h_v, int64_t *index);
+/* IF[j + i*M] (configurationsMap.h:309-344, setupFocks), nc*M int32. */
+MCPI_API int mcpi_focks(mcpi_space sp, int32_t *d_IF);
+/* Map[i + k*nc + l*M*nc] (configurationsMap.h:348-417, OneOneMap), nc*M*M int32. */
+MCPI_API int mcpi_one_one_map(mcpi_space sp, int32_t *d_map);
+/* Number of int32 entries of MapOT (two_orbital=0, configurationsMap.h:617-664)
+ * or MapTT (two_orbital=1, configurationsMap.h:421-474). */
+MCPI_API int mcpi_two_map_size(mcpi_space sp, int two_orbital, int64_t *entries);
+/* MapOT / MapTT and their strides (configurationsMap.h:668-762 / 478-613);
+ * d_stride: nc int64 entries (the reference's strideC, widened). */
+MCPI_API int mcpi_two_map(mcpi_space sp, int two_orbital, int64_t *d_stride, int32_t *d_map);
+
+/* ---- operators -------------------------------------------------------------- */
+/* Orbital integrals, host arrays: Ho[k*M + l] = Ho(k,l) (M*M complex),
+ * Hint[k + s*M + q*M^2 + l*M^3] (M^4 complex) = coefficient of a+_k a+_s a_q a_l.
+ * variant selects the reference's folding of the two-body sum
+ * (hamiltonianMatrix.h:391-416 vs :1370-1418); both agree when Hint has the
+ * bosonic 8-fold symmetry. Builds the forward and adjoint pair operators. */
+MCPI_API int mcpi_set_integrals(mcpi_space sp, const double *h_Ho, const double *h_Hint, int variant);
+/* out = H C (hamiltonianMatrix.h:891-1425 applyHconf_XX semantics; _omp, _X and
+ * the CUDA applyHconf kernel compute the same; MCPI_VARIANT_HASH gives applyHconf). */
+MCPI_API int mcpi_apply_h(mcpi_space sp, const void *d_C, void *d_out);
+/* out = H^dagger C (adjoint of the operator above; equal to H C when Ho is
+ * Hermitian and Hint has the 8-fold symmetry). No reference counterpart. */
+MCPI_API int mcpi_apply_h_adjoint(mcpi_space sp, const void *d_C, void *d_out);
+/* rho1[k*M + l] = <a+_k a_l> (onebodyMatrix.h:190-251, OBrho_XM), device output M*M. */
+MCPI_API int mcpi_rho1(mcpi_space sp, const void *d_C, void *d_rho1);
+/* rho2[k + s*M + q*M^2 + l*M^3] = <a+_k a+_s a_q a_l> (twobodyMatrix.h:991-1487, TBrho_XX). */
+MCPI_API int mcpi_rho2(mcpi_space sp, const void *d_C, void *d_rho2);
+/* Transition densities <phi|a+_k a_l|psi> (t1[k*M + l]) and
+ * <phi|a+_k a+_s a_q a_l|psi> (t2, rho2 layout): every entry reduced, valid for
+ * phi != psi. Generalise OBrho_XM / TBrho_XX; no reference counterpart. */
+MCPI_API int mcpi_trans_rho1(mcpi_space sp, const void *d_phi, const void *d_psi, void *d_t1);
+MCPI_API int mcpi_trans_rho2(mcpi_space sp, const void *d_phi, const void *d_psi, void *d_t2);
+/* <a, b> = sum conj(a) b (groundStateLieb.c:73-85, carrDot), host result. */
+MCPI_API int mcpi_dot(mcpi_space sp, const void *d_a, const void *d_b, double *h_result2);
+
+/* ---- Lanczos (groundStateLieb.c:217-471) ------------------------------------ */
+/* Lanczos with full classical Gram-Schmidt reorthogonalisation
+ * (groundStateLieb.c:217-344, lanczos). d_lvec holds lm vectors of nc complex,
+ * d_lvec[0..nc) = start vector on entry. h_diag (lm complex, alpha) and
+ * h_offdiag (lm doubles, beta) receive the tridiagonal; *iters the number of
+ * steps done (lm, or the step of a breakdown beta_i/max beta < 1e-15). */
+MCPI_API int mcpi_lanczos(mcpi_space sp, void *d_lvec, int lm, double *h_diag, double *h_offdiag,
+                 int *iters);
+/* Lowest eigenpair of H from niter Lanczos steps started at d_C
+ * (groundStateLieb.c:348-471, ground). d_C receives the Ritz vector; *E0 the
+ * eigenvalue. Allocates the niter*nc Krylov basis internally. */
+MCPI_API int mcpi_ground(mcpi_space sp, void *d_C, int niter, double *E0, int *iters);
+/* Eigenvalues (ascending, into d) and optionally row-major eigenvectors
+ * z[k*n + j] of the symmetric tridiagonal (d, e): the LAPACKE_dstev('V') contract
+ * used at groundStateLieb.c:435. Host arrays. */
+MCPI_API int mcpi_tridiag_eig(int n, double *d, double *e, double *z);
+
+/* ---- model inputs ------------------------------------------------------------ */
+/* Lieb-Liniger plane-wave integrals on a ring of length L
+ * (groundStateLieb.c:129-213, setupHo / setupHint), host outputs. */
+MCPI_API int mcpi_lieb_integrals(int M, double g, double L, double *h_Ho, double *h_Hint);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MCPI_B200_H */

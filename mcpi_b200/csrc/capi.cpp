@@ -1,0 +1,711 @@
+// C ABI of libmcpi_b200.so: space contexts, the pair-operator planner and the
+// host side of the Lanczos solver. Declarations: include/mcpi_b200.h.
+#include "../../include/mcpi_b200.h"
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <complex>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "fock.cuh"
+#include "kernels.h"
+
+namespace mcpi {
+int tridiag_eig(int n, double *d, const double *e, double *z);
+}
+
+using mcpi::PairOp;
+using mcpi::Space;
+using mcpi::SpaceTables;
+using cplx = std::complex<double>;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+#define CK(call)                                                                           \
+    do {                                                                                   \
+        cudaError_t _e = (call);                                                           \
+        if (_e != cudaSuccess)                                                             \
+            return fail(_e == cudaErrorMemoryAllocation ? MCPI_ERR_NOMEM : MCPI_ERR_CUDA,  \
+                        "%s failed: %s", #call, cudaGetErrorString(_e));                   \
+    } while (0)
+
+#define CHECK_ARG(cond, msg)                                   \
+    do {                                                       \
+        if (!(cond)) return fail(MCPI_ERR_ARG, "%s", (msg));   \
+    } while (0)
+
+// Exact binomial C(n, k) in 128 bits (n small enough for every use here).
+unsigned __int128 binom128(int64_t n, int64_t k)
+{
+    if (k < 0 || n < 0 || k > n) return 0;
+    if (k > n - k) k = n - k;
+    unsigned __int128 r = 1;
+    for (int64_t i = 1; i <= k; ++i) r = r * (unsigned __int128)(n - k + i) / (unsigned __int128)i;
+    return r;
+}
+
+int64_t nc_exact(int N, int M)  // -1 when it does not fit in 63 bits
+{
+    if (N < 0 || M < 1) return 0;
+    unsigned __int128 r = binom128((int64_t)N + M - 1, N);
+    return r > (unsigned __int128)INT64_MAX ? -1 : (int64_t)r;
+}
+
+// Restores the caller's current device on scope exit.
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev)
+    {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard()
+    {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+struct DevPairOp {
+    int *rowptr = nullptr;
+    uint16_t *col = nullptr;
+    double2 *val = nullptr;
+    double2 *hdiag = nullptr;
+    double2 *hfull = nullptr;
+    int nnz = 0;
+    PairOp view() const { return PairOp{rowptr, col, val, hdiag, hfull, nnz}; }
+};
+
+}  // namespace
+
+struct mcpi_space_s {
+    int N = 0, M = 0, device = 0;
+    Space sp{};
+    int64_t nc = 0, nc1 = 0, nc2 = 0;
+    int P = 0;
+    cudaStream_t own = nullptr, stream = nullptr;
+    uint32_t *d_W = nullptr;
+    double *d_sq = nullptr;
+    bool has_op = false;
+    DevPairOp fwd, adj;
+    double2 *d_E = nullptr;          // P * nc2 scratch of H.psi
+    double2 *d_gram = nullptr;       // density partials
+    size_t gram_cap = 0;
+    double2 *d_dot = nullptr;        // 1 result + partials
+    SpaceTables tables() const { return SpaceTables{d_W, d_sq}; }
+};
+
+namespace {
+
+void free_op(DevPairOp &o)
+{
+    cudaFree(o.rowptr);
+    cudaFree(o.col);
+    cudaFree(o.val);
+    cudaFree(o.hdiag);
+    cudaFree(o.hfull);
+    o = DevPairOp{};
+}
+
+// Pair matrix Ht[a][b] (a = (k<=s) creation pair, b = (q<=l) annihilation
+// pair) such that  sum_ab Ht[a][b] a+_k a+_s a_q a_l  equals the reference's
+// two-body sum rule by rule (hamiltonianMatrix.h:976-1418; each rule's factor
+// 1, 2 or 4 times the outer 1/2, on the Hint entry that rule reads), plus the
+// off-diagonal one-body part folded in as a+_k a_l = (N-1)^-1 sum_s a+_k a+_s a_s a_l.
+std::vector<cplx> build_pair_matrix(int N, int M, const cplx *Ho, const cplx *Hint, int variant)
+{
+    const int P = M * (M + 1) / 2;
+    const size_t M2 = (size_t)M * M, M3 = M2 * M;
+    std::vector<cplx> Ht((size_t)P * P, cplx(0.0, 0.0));
+    auto H = [&](int k, int s, int q, int l) { return Hint[k + s * M + q * M2 + l * M3]; };
+    auto pr = [&](int a, int b) { return a <= b ? mcpi::pair_index(a, b, M) : mcpi::pair_index(b, a, M); };
+    auto at = [&](int a, int b) -> cplx & { return Ht[(size_t)a * P + b]; };
+    if (N >= 2) {
+        for (int k = 0; k < M; ++k) at(pr(k, k), pr(k, k)) += 0.5 * H(k, k, k, k);           // R1
+        for (int k = 0; k < M; ++k)                                                           // R2
+            for (int s = k + 1; s < M; ++s) at(pr(k, s), pr(k, s)) += 2.0 * H(k, s, k, s);
+        for (int k = 0; k < M; ++k)                                                           // R3
+            for (int q = 0; q < M; ++q)
+                if (q != k) at(pr(k, k), pr(q, q)) += 0.5 * H(k, k, q, q);
+        for (int k = 0; k < M; ++k)                                                           // R4
+            for (int l = 0; l < M; ++l)
+                if (l != k) at(pr(k, k), pr(k, l)) += H(k, k, k, l);
+        for (int k = 0; k < M; ++k)                                                           // R5
+            for (int s = 0; s < M; ++s)
+                if (s != k) at(pr(k, s), pr(s, s)) += H(k, s, s, s);
+        for (int k = 0; k < M; ++k)                                                           // R6
+            for (int q = 0; q < M; ++q)
+                for (int l = q + 1; l < M; ++l)
+                    if (q != k && l != k) at(pr(k, k), pr(q, l)) += H(k, k, q, l);
+        for (int k = 0; k < M; ++k)                                                           // R7
+            for (int s = k + 1; s < M; ++s)
+                for (int q = 0; q < M; ++q)
+                    if (q != k && q != s) at(pr(k, s), pr(q, q)) += H(k, s, q, q);
+        for (int s = 0; s < M; ++s)                                                           // R8
+            for (int k = 0; k < M; ++k)
+                for (int l = 0; l < M; ++l)
+                    if (k != s && l != k && l != s) at(pr(k, s), pr(s, l)) += 2.0 * H(k, s, s, l);
+        for (int k = 0; k < M; ++k)                                                           // R9
+            for (int s = k + 1; s < M; ++s)
+                for (int q = 0; q < M; ++q)
+                    for (int l = q + 1; l < M; ++l) {
+                        if (q == k || q == s || l == k || l == s) continue;
+                        if (variant == MCPI_VARIANT_HASH)
+                            at(pr(k, s), pr(q, l)) +=
+                                0.5 * (H(k, s, q, l) + H(s, k, q, l) + H(k, s, l, q) + H(s, k, l, q));
+                        else
+                            at(pr(k, s), pr(q, l)) += 2.0 * H(k, s, q, l);
+                    }
+        // off-diagonal one-body, folded
+        const double f = 1.0 / (N - 1);
+        for (int k = 0; k < M; ++k)
+            for (int l = 0; l < M; ++l) {
+                if (k == l || Ho[k * M + l] == cplx(0.0, 0.0)) continue;
+                for (int s = 0; s < M; ++s) at(pr(k, s), pr(s, l)) += f * Ho[k * M + l];
+            }
+    }
+    return Ht;
+}
+
+int upload_op(mcpi_space_s *sp, DevPairOp &op, const std::vector<cplx> &Ht, const cplx *hdiag,
+              const cplx *hfull)
+{
+    const int P = sp->P, M = sp->M;
+    std::vector<int> rowptr(P + 1, 0);
+    std::vector<uint16_t> col;
+    std::vector<cplx> val;
+    for (int a = 0; a < P; ++a) {
+        for (int b = 0; b < P; ++b) {
+            const cplx h = Ht[(size_t)a * P + b];
+            if (h != cplx(0.0, 0.0)) {
+                col.push_back((uint16_t)b);
+                val.push_back(h);
+            }
+        }
+        rowptr[a + 1] = (int)col.size();
+    }
+    free_op(op);
+    const size_t nnz = col.size() ? col.size() : 1;
+    CK(cudaMalloc(&op.rowptr, sizeof(int) * (P + 1)));
+    CK(cudaMalloc(&op.col, sizeof(uint16_t) * nnz));
+    CK(cudaMalloc(&op.val, sizeof(double2) * nnz));
+    CK(cudaMalloc(&op.hdiag, sizeof(double2) * M));
+    CK(cudaMalloc(&op.hfull, sizeof(double2) * M * M));
+    CK(cudaMemcpyAsync(op.rowptr, rowptr.data(), sizeof(int) * (P + 1), cudaMemcpyHostToDevice, sp->stream));
+    if (!col.empty()) {
+        CK(cudaMemcpyAsync(op.col, col.data(), sizeof(uint16_t) * col.size(), cudaMemcpyHostToDevice, sp->stream));
+        CK(cudaMemcpyAsync(op.val, val.data(), sizeof(double2) * val.size(), cudaMemcpyHostToDevice, sp->stream));
+    }
+    CK(cudaMemcpyAsync(op.hdiag, hdiag, sizeof(double2) * M, cudaMemcpyHostToDevice, sp->stream));
+    CK(cudaMemcpyAsync(op.hfull, hfull, sizeof(double2) * M * M, cudaMemcpyHostToDevice, sp->stream));
+    CK(cudaStreamSynchronize(sp->stream));  // host vectors go out of scope
+    op.nnz = (int)col.size();
+    return MCPI_OK;
+}
+
+int ensure_E(mcpi_space_s *sp)
+{
+    if (sp->N < 2 || sp->d_E) return MCPI_OK;
+    CK(cudaMalloc(&sp->d_E, sizeof(double2) * (size_t)sp->P * sp->nc2));
+    return MCPI_OK;
+}
+
+int ensure_gram(mcpi_space_s *sp)
+{
+    const size_t need = mcpi::gram_partial_elems(sp->sp, 2) > mcpi::gram_partial_elems(sp->sp, 1)
+                            ? mcpi::gram_partial_elems(sp->sp, 2)
+                            : mcpi::gram_partial_elems(sp->sp, 1);
+    if (sp->gram_cap >= need) return MCPI_OK;
+    cudaFree(sp->d_gram);
+    sp->d_gram = nullptr;
+    CK(cudaMalloc(&sp->d_gram, sizeof(double2) * need));
+    sp->gram_cap = need;
+    return MCPI_OK;
+}
+
+int apply_op(mcpi_space_s *sp, const DevPairOp &op, const void *d_C, void *d_out)
+{
+    CHECK_ARG(sp && d_C && d_out, "null argument");
+    if (!sp->has_op) return fail(MCPI_ERR_STATE, "mcpi_set_integrals has not been called");
+    CHECK_ARG(d_C != d_out, "input and output must not alias");
+    DeviceGuard g(sp->device);
+    int rc = ensure_E(sp);
+    if (rc) return rc;
+    CK(mcpi::launch_apply_h(sp->sp, sp->tables(), op.view(), (const double2 *)d_C, sp->d_E,
+                            (double2 *)d_out, sp->stream));
+    return MCPI_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *mcpi_status_string(int status)
+{
+    switch (status) {
+    case MCPI_OK: return "ok";
+    case MCPI_ERR_ARG: return "invalid argument";
+    case MCPI_ERR_RANGE: return "size out of supported range";
+    case MCPI_ERR_CUDA: return "CUDA error";
+    case MCPI_ERR_NOMEM: return "out of memory";
+    case MCPI_ERR_STATE: return "invalid call order";
+    case MCPI_ERR_NUMERIC: return "numerical failure";
+    default: return "unknown status";
+    }
+}
+
+const char *mcpi_last_error(void) { return g_last_error.c_str(); }
+
+int mcpi_nc(int N, int M, int64_t *nc)
+{
+    CHECK_ARG(nc && N >= 0 && M >= 1, "mcpi_nc: need N >= 0, M >= 1");
+    const int64_t v = nc_exact(N, M);
+    if (v < 0) return fail(MCPI_ERR_RANGE, "NC(%d,%d) exceeds 63 bits", N, M);
+    *nc = v;
+    return MCPI_OK;
+}
+
+int mcpi_space_create(int N, int M, int device, mcpi_space *out)
+{
+    CHECK_ARG(out, "null output");
+    *out = nullptr;
+    CHECK_ARG(N >= 0 && M >= 1, "need N >= 0 and M >= 1");
+    if (M > mcpi::kMaxM) return fail(MCPI_ERR_RANGE, "M=%d exceeds the supported %d orbitals", M, mcpi::kMaxM);
+    const int64_t nc = nc_exact(N, M);
+    if (nc < 0 || nc >= (int64_t)1 << 31)
+        return fail(MCPI_ERR_RANGE, "NC(%d,%d) does not fit the 31-bit configuration index", N, M);
+    const int ws = N + 3;
+    if ((size_t)(M - 1) * ws * 4 + (size_t)ws * 8 > 24 * 1024)
+        return fail(MCPI_ERR_RANGE, "N=%d too large for the shared-memory binomial table", N);
+    int ndev = 0;
+    CK(cudaGetDeviceCount(&ndev));
+    CHECK_ARG(device >= 0 && device < ndev, "invalid device ordinal");
+    DeviceGuard g(device);
+    auto *s = new mcpi_space_s;
+    s->N = N;
+    s->M = M;
+    s->device = device;
+    s->nc = nc;
+    s->nc1 = N >= 1 ? nc_exact(N - 1, M) : 0;
+    s->nc2 = N >= 2 ? nc_exact(N - 2, M) : 0;
+    s->P = M * (M + 1) / 2;
+    s->sp.N = N;
+    s->sp.M = M;
+    s->sp.wstride = ws;
+    s->sp.nc = (uint32_t)nc;
+    s->sp.nc1 = (uint32_t)s->nc1;
+    s->sp.nc2 = (uint32_t)s->nc2;
+    // W[i*ws + p] = C(p+i, i+1) mod 2^32, from Pascal's triangle mod 2^64 (exact modular)
+    const int nmax = N + 2 + M;
+    std::vector<std::vector<uint64_t>> C(nmax + 1, std::vector<uint64_t>(nmax + 1, 0));
+    for (int n = 0; n <= nmax; ++n) {
+        C[n][0] = 1;
+        for (int k = 1; k <= n; ++k) C[n][k] = C[n - 1][k - 1] + (k <= n - 1 ? C[n - 1][k] : 0);
+    }
+    std::vector<uint32_t> W((size_t)(M > 1 ? M - 1 : 1) * ws, 0);
+    for (int i = 0; i + 1 < M; ++i)
+        for (int p = 0; p < ws; ++p) W[(size_t)i * ws + p] = (uint32_t)C[p + i][i + 1];
+    std::vector<double> sq(ws);
+    for (int n = 0; n < ws; ++n) sq[n] = std::sqrt((double)n);
+    cudaError_t e = cudaStreamCreateWithFlags(&s->own, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&s->d_W, sizeof(uint32_t) * W.size());
+    if (e == cudaSuccess) e = cudaMalloc(&s->d_sq, sizeof(double) * ws);
+    if (e == cudaSuccess) e = cudaMalloc(&s->d_dot, sizeof(double2) * (mcpi::lanczos_parts(nc) + 1));
+    if (e == cudaSuccess) e = cudaMemcpy(s->d_W, W.data(), sizeof(uint32_t) * W.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(s->d_sq, sq.data(), sizeof(double) * ws, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        mcpi_space_destroy(s);
+        return fail(e == cudaErrorMemoryAllocation ? MCPI_ERR_NOMEM : MCPI_ERR_CUDA,
+                    "mcpi_space_create: %s", cudaGetErrorString(e));
+    }
+    s->stream = s->own;
+    *out = s;
+    return MCPI_OK;
+}
+
+int mcpi_space_destroy(mcpi_space sp)
+{
+    if (!sp) return MCPI_OK;
+    DeviceGuard g(sp->device);
+    if (sp->stream) cudaStreamSynchronize(sp->stream);
+    free_op(sp->fwd);
+    free_op(sp->adj);
+    cudaFree(sp->d_W);
+    cudaFree(sp->d_sq);
+    cudaFree(sp->d_E);
+    cudaFree(sp->d_gram);
+    cudaFree(sp->d_dot);
+    if (sp->own) cudaStreamDestroy(sp->own);
+    delete sp;
+    return MCPI_OK;
+}
+
+int mcpi_space_set_stream(mcpi_space sp, void *stream)
+{
+    CHECK_ARG(sp, "null space");
+    sp->stream = (cudaStream_t)stream;   // NULL selects the legacy default stream
+    return MCPI_OK;
+}
+
+int mcpi_space_sync(mcpi_space sp)
+{
+    CHECK_ARG(sp, "null space");
+    DeviceGuard g(sp->device);
+    CK(cudaStreamSynchronize(sp->stream));
+    return MCPI_OK;
+}
+
+int mcpi_space_dims(mcpi_space sp, int *N, int *M, int64_t *nc)
+{
+    CHECK_ARG(sp, "null space");
+    if (N) *N = sp->N;
+    if (M) *M = sp->M;
+    if (nc) *nc = sp->nc;
+    return MCPI_OK;
+}
+
+// ---- tables -----------------------------------------------------------------
+
+int mcpi_ncmat(int N, int M, int32_t *h)
+{
+    CHECK_ARG(h && N >= 0 && M >= 1, "mcpi_ncmat: bad arguments");
+    for (int n = 0; n <= N; ++n) {
+        h[n] = 0;
+        if (M >= 1) h[n + (N + 1)] = 1;
+        for (int m = 2; m <= M; ++m) {
+            const int64_t v = nc_exact(n, m);
+            if (v < 0 || v > INT32_MAX) return fail(MCPI_ERR_RANGE, "NC(%d,%d) exceeds int32", n, m);
+            h[n + (N + 1) * m] = (int32_t)v;
+        }
+    }
+    return MCPI_OK;
+}
+
+int mcpi_index_to_fock(int N, int M, int64_t index, int32_t *v)
+{
+    CHECK_ARG(v && N >= 0 && M >= 1 && M <= 64, "mcpi_index_to_fock: bad arguments");
+    const int64_t nc = nc_exact(N, M);
+    CHECK_ARG(nc > 0 && index >= 0 && index < nc, "index out of range");
+    // R = NC(N,M) - 1 - index = sum_i C(P_i + i, i+1); greedy from the top orbital
+    unsigned __int128 R = (unsigned __int128)(nc - 1 - index);
+    int hi = N;
+    std::vector<int> P(M);
+    P[M - 1] = N;
+    for (int i = M - 2; i >= 0; --i) {
+        int p = hi;
+        while (p > 0 && binom128(p + i, i + 1) > R) --p;
+        R -= binom128(p + i, i + 1);
+        P[i] = p;
+        hi = p;
+    }
+    v[0] = P[0];
+    for (int i = 1; i < M; ++i) v[i] = P[i] - P[i - 1];
+    return MCPI_OK;
+}
+
+int mcpi_fock_to_index(int N, int M, const int32_t *v, int64_t *index)
+{
+    CHECK_ARG(v && index && N >= 0 && M >= 1, "mcpi_fock_to_index: bad arguments");
+    int64_t tot = 0;
+    for (int i = 0; i < M; ++i) {
+        CHECK_ARG(v[i] >= 0, "negative occupation");
+        tot += v[i];
+    }
+    CHECK_ARG(tot == N, "occupations do not sum to N");
+    unsigned __int128 s = 0;
+    int64_t P = 0;
+    for (int i = 0; i + 1 < M; ++i) {
+        P += v[i];
+        s += binom128(P + i, i + 1);
+    }
+    *index = nc_exact(N, M) - 1 - (int64_t)s;
+    return MCPI_OK;
+}
+
+int mcpi_focks(mcpi_space sp, int32_t *d_IF)
+{
+    CHECK_ARG(sp && d_IF, "null argument");
+    DeviceGuard g(sp->device);
+    CK(mcpi::launch_focks(sp->sp, sp->tables(), d_IF, sp->stream));
+    return MCPI_OK;
+}
+
+int mcpi_one_one_map(mcpi_space sp, int32_t *d_map)
+{
+    CHECK_ARG(sp && d_map, "null argument");
+    DeviceGuard g(sp->device);
+    CK(mcpi::launch_one_one_map(sp->sp, sp->tables(), d_map, sp->stream));
+    return MCPI_OK;
+}
+
+int mcpi_two_map_size(mcpi_space sp, int two_orbital, int64_t *entries)
+{
+    CHECK_ARG(sp && entries, "null argument");
+    DeviceGuard g(sp->device);
+    int64_t *cnt = nullptr, *stride = nullptr, *tot = nullptr;
+    void *scratch = nullptr;
+    size_t need = 0;
+    int rc = MCPI_OK;
+    cudaError_t e = cudaMalloc(&cnt, sizeof(int64_t) * sp->nc);
+    if (e == cudaSuccess) e = cudaMalloc(&stride, sizeof(int64_t) * sp->nc);
+    if (e == cudaSuccess) e = cudaMalloc(&tot, sizeof(int64_t));
+    if (e == cudaSuccess) e = mcpi::launch_chunk_counts(sp->sp, sp->tables(), two_orbital, cnt, sp->stream);
+    if (e == cudaSuccess) e = mcpi::launch_stride_scan(sp->sp, cnt, stride, tot, nullptr, 0, &need, sp->stream);
+    if (e == cudaSuccess) e = cudaMalloc(&scratch, need ? need : 1);
+    if (e == cudaSuccess) e = mcpi::launch_stride_scan(sp->sp, cnt, stride, tot, scratch, need, nullptr, sp->stream);
+    int64_t chunks = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&chunks, tot, sizeof(int64_t), cudaMemcpyDeviceToHost, sp->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(sp->stream);
+    if (e != cudaSuccess) rc = fail(MCPI_ERR_CUDA, "mcpi_two_map_size: %s", cudaGetErrorString(e));
+    else *entries = chunks * sp->M * sp->M;
+    cudaFree(cnt);
+    cudaFree(stride);
+    cudaFree(tot);
+    cudaFree(scratch);
+    return rc;
+}
+
+int mcpi_two_map(mcpi_space sp, int two_orbital, int64_t *d_stride, int32_t *d_map)
+{
+    CHECK_ARG(sp && d_stride && d_map, "null argument");
+    DeviceGuard g(sp->device);
+    int64_t *cnt = nullptr, *tot = nullptr;
+    void *scratch = nullptr;
+    size_t need = 0;
+    int rc = MCPI_OK;
+    cudaError_t e = cudaMalloc(&cnt, sizeof(int64_t) * sp->nc);
+    if (e == cudaSuccess) e = cudaMalloc(&tot, sizeof(int64_t));
+    if (e == cudaSuccess) e = mcpi::launch_chunk_counts(sp->sp, sp->tables(), two_orbital, cnt, sp->stream);
+    if (e == cudaSuccess) e = mcpi::launch_stride_scan(sp->sp, cnt, d_stride, tot, nullptr, 0, &need, sp->stream);
+    if (e == cudaSuccess) e = cudaMalloc(&scratch, need ? need : 1);
+    if (e == cudaSuccess) e = mcpi::launch_stride_scan(sp->sp, cnt, d_stride, tot, scratch, need, nullptr, sp->stream);
+    if (e == cudaSuccess) e = mcpi::launch_two_map(sp->sp, sp->tables(), two_orbital, d_stride, d_map, sp->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(sp->stream);
+    if (e != cudaSuccess) rc = fail(MCPI_ERR_CUDA, "mcpi_two_map: %s", cudaGetErrorString(e));
+    cudaFree(cnt);
+    cudaFree(tot);
+    cudaFree(scratch);
+    return rc;
+}
+
+// ---- operators -------------------------------------------------------------------
+
+int mcpi_set_integrals(mcpi_space sp, const double *h_Ho, const double *h_Hint, int variant)
+{
+    CHECK_ARG(sp && h_Ho && h_Hint, "null argument");
+    CHECK_ARG(variant == MCPI_VARIANT_MAPS || variant == MCPI_VARIANT_HASH, "unknown variant");
+    DeviceGuard g(sp->device);
+    const int M = sp->M, P = sp->P;
+    const cplx *Ho = reinterpret_cast<const cplx *>(h_Ho);
+    const cplx *Hint = reinterpret_cast<const cplx *>(h_Hint);
+    std::vector<cplx> Ht = build_pair_matrix(sp->N, M, Ho, Hint, variant);
+    std::vector<cplx> hd(M), hf(Ho, Ho + (size_t)M * M), hda(M), hfa((size_t)M * M);
+    for (int k = 0; k < M; ++k) {
+        hd[k] = Ho[k * M + k];
+        hda[k] = std::conj(hd[k]);
+        for (int l = 0; l < M; ++l) hfa[k * M + l] = std::conj(Ho[l * M + k]);
+    }
+    std::vector<cplx> Hta((size_t)P * P);
+    for (int a = 0; a < P; ++a)
+        for (int b = 0; b < P; ++b) Hta[(size_t)b * P + a] = std::conj(Ht[(size_t)a * P + b]);
+    int rc = upload_op(sp, sp->fwd, Ht, hd.data(), hf.data());
+    if (rc) return rc;
+    rc = upload_op(sp, sp->adj, Hta, hda.data(), hfa.data());
+    if (rc) return rc;
+    sp->has_op = true;
+    return MCPI_OK;
+}
+
+int mcpi_apply_h(mcpi_space sp, const void *d_C, void *d_out) { return apply_op(sp, sp ? sp->fwd : DevPairOp{}, d_C, d_out); }
+
+int mcpi_apply_h_adjoint(mcpi_space sp, const void *d_C, void *d_out)
+{
+    return apply_op(sp, sp ? sp->adj : DevPairOp{}, d_C, d_out);
+}
+
+static int density(mcpi_space sp, int order, const void *phi, const void *psi, void *out)
+{
+    CHECK_ARG(sp && phi && psi && out, "null argument");
+    DeviceGuard g(sp->device);
+    int rc = ensure_gram(sp);
+    if (rc) return rc;
+    CK(mcpi::launch_density(sp->sp, sp->tables(), order, (const double2 *)phi, (const double2 *)psi,
+                            sp->d_gram, (double2 *)out, sp->stream));
+    return MCPI_OK;
+}
+
+int mcpi_rho1(mcpi_space sp, const void *d_C, void *d_rho1) { return density(sp, 1, d_C, d_C, d_rho1); }
+int mcpi_rho2(mcpi_space sp, const void *d_C, void *d_rho2) { return density(sp, 2, d_C, d_C, d_rho2); }
+int mcpi_trans_rho1(mcpi_space sp, const void *phi, const void *psi, void *t1) { return density(sp, 1, phi, psi, t1); }
+int mcpi_trans_rho2(mcpi_space sp, const void *phi, const void *psi, void *t2) { return density(sp, 2, phi, psi, t2); }
+
+int mcpi_dot(mcpi_space sp, const void *d_a, const void *d_b, double *h_result2)
+{
+    CHECK_ARG(sp && d_a && d_b && h_result2, "null argument");
+    DeviceGuard g(sp->device);
+    CK(mcpi::launch_dot((const double2 *)d_a, (const double2 *)d_b, sp->nc, sp->d_dot + 1, sp->d_dot,
+                        sp->stream));
+    CK(cudaMemcpyAsync(h_result2, sp->d_dot, sizeof(double2), cudaMemcpyDeviceToHost, sp->stream));
+    CK(cudaStreamSynchronize(sp->stream));
+    return MCPI_OK;
+}
+
+// ---- Lanczos -------------------------------------------------------------------------
+
+int mcpi_lanczos(mcpi_space sp, void *d_lvec, int lm, double *h_diag, double *h_offdiag, int *iters)
+{
+    CHECK_ARG(sp && d_lvec && lm >= 1, "mcpi_lanczos: bad arguments");
+    if (!sp->has_op) return fail(MCPI_ERR_STATE, "mcpi_set_integrals has not been called");
+    DeviceGuard g(sp->device);
+    int rc = ensure_E(sp);
+    if (rc) return rc;
+    const int64_t nc = sp->nc;
+    const size_t npart = mcpi::lanczos_partial_elems(nc, lm);
+    // state block: alpha(lm) coef(lm) partial(npart) | beta(lm) maxbeta | done iters
+    char *blk = nullptr;
+    const size_t bytes = sizeof(double2) * (2 * (size_t)lm + npart) + sizeof(double) * (lm + 1) + 2 * sizeof(int);
+    double2 *r = nullptr;
+    CK(cudaMalloc(&blk, bytes));
+    cudaError_t e = cudaMalloc(&r, sizeof(double2) * nc);
+    if (e != cudaSuccess) {
+        cudaFree(blk);
+        return fail(MCPI_ERR_NOMEM, "mcpi_lanczos: %s", cudaGetErrorString(e));
+    }
+    mcpi::LanczosState s;
+    s.alpha = (double2 *)blk;
+    s.coef = s.alpha + lm;
+    s.partial = s.coef + lm;
+    s.beta = (double *)(s.partial + npart);
+    s.maxbeta = s.beta + lm;
+    s.done = (int *)(s.maxbeta + 1);
+    s.iters = s.done + 1;
+    s.nparts = mcpi::lanczos_parts(nc);
+    const int init[2] = {0, lm};
+    double2 *V = (double2 *)d_lvec;
+    const PairOp op = sp->fwd.view();
+    const SpaceTables tb = sp->tables();
+    e = cudaMemsetAsync(blk, 0, bytes, sp->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(s.done, init, sizeof init, cudaMemcpyHostToDevice, sp->stream);
+    if (e == cudaSuccess) e = mcpi::launch_apply_h(sp->sp, tb, op, V, sp->d_E, r, sp->stream);
+    if (e == cudaSuccess) e = mcpi::launch_lanczos_start(V, r, r, nc, s, sp->stream);
+    for (int i = 0; i < lm - 1 && e == cudaSuccess; ++i) {
+        double2 *vi = V + (size_t)i * nc, *vn = V + (size_t)(i + 1) * nc;
+        e = mcpi::launch_lanczos_beta(i, lm, 1e-15, s, sp->stream);
+        if (e == cudaSuccess) e = mcpi::launch_lanczos_scale(r, vn, nc, i, s, sp->stream);
+        if (e == cudaSuccess) e = mcpi::launch_apply_h(sp->sp, tb, op, vn, sp->d_E, r, sp->stream);
+        if (e == cudaSuccess) e = mcpi::launch_lanczos_alpha(vi, vn, r, nc, i, s, sp->stream);
+        if (e == cudaSuccess) e = mcpi::launch_lanczos_reorth(V, i + 2, r, nc, i, s, sp->stream);
+    }
+    std::vector<double2> alpha(lm);
+    std::vector<double> beta(lm);
+    int it = lm;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(alpha.data(), s.alpha, sizeof(double2) * lm, cudaMemcpyDeviceToHost, sp->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(beta.data(), s.beta, sizeof(double) * lm, cudaMemcpyDeviceToHost, sp->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&it, s.iters, sizeof(int), cudaMemcpyDeviceToHost, sp->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(sp->stream);
+    cudaFree(blk);
+    cudaFree(r);
+    if (e != cudaSuccess) return fail(MCPI_ERR_CUDA, "mcpi_lanczos: %s", cudaGetErrorString(e));
+    if (h_diag) std::memcpy(h_diag, alpha.data(), sizeof(double2) * lm);
+    if (h_offdiag) {
+        for (int i = 0; i < lm; ++i) h_offdiag[i] = i < lm - 1 ? beta[i] : 0.0;
+    }
+    if (iters) *iters = it;
+    return MCPI_OK;
+}
+
+int mcpi_tridiag_eig(int n, double *d, double *e, double *z)
+{
+    CHECK_ARG(n >= 0 && (n == 0 || (d && (n == 1 || e))), "mcpi_tridiag_eig: bad arguments");
+    if (mcpi::tridiag_eig(n, d, e, z) != 0) return fail(MCPI_ERR_NUMERIC, "tridiagonal QL did not converge");
+    return MCPI_OK;
+}
+
+int mcpi_ground(mcpi_space sp, void *d_C, int niter, double *E0, int *iters)
+{
+    CHECK_ARG(sp && d_C && E0 && niter >= 1, "mcpi_ground: bad arguments");
+    DeviceGuard g(sp->device);
+    const int64_t nc = sp->nc;
+    double2 *V = nullptr;
+    CK(cudaMalloc(&V, sizeof(double2) * nc * (size_t)niter));
+    cudaError_t e = cudaMemcpyAsync(V, d_C, sizeof(double2) * nc, cudaMemcpyDeviceToDevice, sp->stream);
+    if (e != cudaSuccess) {
+        cudaFree(V);
+        return fail(MCPI_ERR_CUDA, "mcpi_ground: %s", cudaGetErrorString(e));
+    }
+    std::vector<double> diag(2 * (size_t)niter), off(niter);
+    int it = 0;
+    int rc = mcpi_lanczos(sp, V, niter, diag.data(), off.data(), &it);
+    if (rc) {
+        cudaFree(V);
+        return rc;
+    }
+    // groundStateLieb.c:419-449; a breakdown at the first step keeps alpha_0
+    const int n = it > 0 ? it : 1;
+    std::vector<double> d(n), ee(n > 1 ? n - 1 : 1), z((size_t)n * n);
+    for (int k = 0; k < n; ++k) d[k] = diag[2 * k];
+    for (int k = 0; k + 1 < n; ++k) ee[k] = off[k];
+    if (mcpi::tridiag_eig(n, d.data(), ee.data(), z.data()) != 0) {
+        cudaFree(V);
+        return fail(MCPI_ERR_NUMERIC, "tridiagonal QL did not converge");
+    }
+    double sentinel = 1e10;
+    int jmin = 0;
+    for (int k = 0; k < n; ++k)
+        if (sentinel > d[k]) {
+            sentinel = d[k];
+            jmin = k;
+        }
+    std::vector<double> zc(n);
+    for (int k = 0; k < n; ++k) zc[k] = z[(size_t)k * n + jmin];
+    double *dz = nullptr;
+    e = cudaMalloc(&dz, sizeof(double) * n);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dz, zc.data(), sizeof(double) * n, cudaMemcpyHostToDevice, sp->stream);
+    if (e == cudaSuccess) e = mcpi::launch_combine(V, n, nc, dz, (double2 *)d_C, sp->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(sp->stream);
+    cudaFree(dz);
+    cudaFree(V);
+    if (e != cudaSuccess) return fail(MCPI_ERR_CUDA, "mcpi_ground: %s", cudaGetErrorString(e));
+    *E0 = d[jmin];
+    if (iters) *iters = it;
+    return MCPI_OK;
+}
+
+int mcpi_lieb_integrals(int M, double g, double L, double *h_Ho, double *h_Hint)
+{
+    CHECK_ARG(M >= 1 && h_Ho && h_Hint && L > 0, "mcpi_lieb_integrals: bad arguments");
+    const double pi = 3.141592653589793;
+    cplx *Ho = reinterpret_cast<cplx *>(h_Ho);
+    cplx *Hint = reinterpret_cast<cplx *>(h_Hint);
+    for (int n = 0; n < M; ++n) {
+        const double k = 2 * pi * (n - M / 2) / L;
+        for (int j = 0; j < M; ++j) Ho[n * M + j] = 0.0;
+        Ho[n * M + n] = 0.5 * k * k;
+    }
+    const size_t M2 = (size_t)M * M, M3 = M2 * M;
+    for (int n = 0; n < M; ++n)
+        for (int s = 0; s < M; ++s)
+            for (int q = 0; q < M; ++q)
+                for (int l = 0; l < M; ++l)
+                    Hint[n + s * M + q * M2 + l * M3] = (l + q - s - n == 0) ? g : 0.0;
+    return MCPI_OK;
+}
+
+}  // extern "C"

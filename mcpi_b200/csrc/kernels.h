@@ -1,0 +1,85 @@
+// Internal launch interface between the C ABI layer (capi.cpp) and the CUDA
+// translation units. Nothing here is part of the public ABI.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "fock.cuh"
+
+namespace mcpi {
+
+// Two-body operator in pair form: H2 = sum_{a,b} Ht[a][b] A+_a A_b with
+// A_b = a_q a_l for the pair b = (q <= l). Stored as CSR over rows a.
+// hdiag[k] = Ho[k][k] (the diagonal one-body part, applied directly);
+// hfull = Ho (M*M, row-major), used only for the one-particle space.
+struct PairOp {
+    const int *rowptr;      // P + 1
+    const uint16_t *col;    // nnz
+    const double2 *val;     // nnz
+    const double2 *hdiag;   // M
+    const double2 *hfull;   // M * M
+    int nnz;
+};
+
+// Device tables of one space.
+struct SpaceTables {
+    const uint32_t *W;      // (M-1) x wstride, W[i*ws + p] = C(p+i, i+1) mod 2^32
+    const double *sq;       // sqrt(n), n = 0 .. N+2
+};
+
+// H.psi : out = H psi. E is scratch of P * nc2 complex (unused when N < 2).
+cudaError_t launch_apply_h(const Space &sp, const SpaceTables &tb, const PairOp &op,
+                           const double2 *psi, double2 *E, double2 *out, cudaStream_t st);
+
+// Densities as Gram matrices over the (N-order)-particle space:
+// G[a][b] = sum_m conj(<m|A_a|phi>) <m|A_b|psi>, expanded to the reference
+// layouts: order 1 -> rho1[k*M + l]; order 2 -> rho2[k + s*M + q*M^2 + l*M^3].
+// partial: scratch of >= gram_partial_elems(sp, order) complex.
+size_t gram_partial_elems(const Space &sp, int order);
+cudaError_t launch_density(const Space &sp, const SpaceTables &tb, int order,
+                           const double2 *phi, const double2 *psi, double2 *partial,
+                           double2 *out, cudaStream_t st);
+
+// Reference-layout tables built on the device.
+cudaError_t launch_focks(const Space &sp, const SpaceTables &tb, int32_t *IF, cudaStream_t st);
+cudaError_t launch_one_one_map(const Space &sp, const SpaceTables &tb, int32_t *Map,
+                               cudaStream_t st);
+// chunk counts per configuration (two_orbital = 0: v_k >= 2; 1: pairs k<s occupied)
+cudaError_t launch_chunk_counts(const Space &sp, const SpaceTables &tb, int two_orbital,
+                                int64_t *counts, cudaStream_t st);
+// exclusive scan of counts * M*M into stride (int64), total chunks to *d_total
+cudaError_t launch_stride_scan(const Space &sp, const int64_t *counts, int64_t *stride,
+                               int64_t *d_total, void *scratch, size_t scratch_bytes,
+                               size_t *scratch_needed, cudaStream_t st);
+cudaError_t launch_two_map(const Space &sp, const SpaceTables &tb, int two_orbital,
+                           const int64_t *stride, int32_t *Map, cudaStream_t st);
+cudaError_t launch_narrow_stride(const int64_t *in, int32_t *out, int64_t n, cudaStream_t st);
+
+// Lanczos vector kernels (all no-ops once *done != 0).
+struct LanczosState {
+    double2 *alpha;      // lm
+    double *beta;        // lm
+    double *maxbeta;     // 1
+    int *done;           // 1
+    int *iters;          // 1 : steps completed (lm unless broken down)
+    double2 *coef;       // lm   : reorthogonalisation coefficients of the current step
+    double2 *partial;    // scratch of lanczos_partial_elems(nc, lm) complex
+    int nparts;          // = lanczos_parts(nc): blocks of the fixed-size reductions
+};
+
+int lanczos_parts(int64_t nc);
+size_t lanczos_partial_elems(int64_t nc, int lm);
+cudaError_t launch_lanczos_start(const double2 *v0, const double2 *hv, double2 *r, int64_t nc,
+                                 LanczosState s, cudaStream_t st);
+cudaError_t launch_lanczos_beta(int i, int lm, double tol, LanczosState s, cudaStream_t st);
+cudaError_t launch_lanczos_scale(const double2 *r, double2 *vnext, int64_t nc, int i,
+                                 LanczosState s, cudaStream_t st);
+cudaError_t launch_lanczos_alpha(const double2 *vprev, const double2 *vcur, double2 *r,
+                                 int64_t nc, int i, LanczosState s, cudaStream_t st);
+cudaError_t launch_lanczos_reorth(const double2 *V, int nvec, double2 *r, int64_t nc, int i,
+                                  LanczosState s, cudaStream_t st);
+cudaError_t launch_combine(const double2 *V, int nvec, int64_t nc, const double *z,
+                           double2 *out, cudaStream_t st);
+cudaError_t launch_dot(const double2 *a, const double2 *b, int64_t nc, double2 *partial,
+                       double2 *result, cudaStream_t st);
+
+}  // namespace mcpi

@@ -1,0 +1,233 @@
+"""Parity of the CUDA path with the reference (golden fixtures) and the oracle.
+
+Bars: tables bit-exact; H.psi, rho1, rho2 and the transition densities within
+1e-12 relative Frobenius error of the reference's FP64 CPU routines; Lanczos
+E0 within 1e-10 (relative to max(1,|E0|)).
+"""
+import numpy as np
+import pytest
+import torch
+
+import mcpi_b200 as mc
+import oracle
+from conftest import case_keys, rel
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+TABLE_NAMES = ["IF", "Map", "MapOT", "strideOT", "MapTT", "strideTT"]
+
+
+def _space(N, M):
+    return mc.FockSpace(N, M, device=0)
+
+
+# ---------------------------------------------------------------- tables ----
+
+def test_tables_bit_exact_golden(golden_tables):
+    cases = sorted({tuple(map(int, k.split("_")[1:])) for k in golden_tables if k.startswith("IF_")})
+    for N, M in cases:
+        sp = _space(N, M)
+        g = {n: golden_tables[f"{n}_{N}_{M}"] for n in TABLE_NAMES}
+        assert np.array_equal(sp.focks().cpu().numpy(), g["IF"]), (N, M)
+        assert np.array_equal(sp.one_one_map().cpu().numpy(), g["Map"]), (N, M)
+        m, s = sp.two_map(False)
+        assert np.array_equal(m.cpu().numpy(), g["MapOT"]) and np.array_equal(s.cpu().numpy(), g["strideOT"])
+        m, s = sp.two_map(True)
+        assert np.array_equal(m.cpu().numpy(), g["MapTT"]) and np.array_equal(s.cpu().numpy(), g["strideTT"])
+        sp.close()
+
+
+@pytest.mark.parametrize("N,M", [(10, 6), (8, 8), (10, 10), (6, 13)])
+def test_tables_bit_exact_oracle(orc, N, M):
+    sp = _space(N, M)
+    IF = orc.focks(N, M)
+    assert np.array_equal(sp.focks().cpu().numpy(), IF)
+    assert np.array_equal(sp.one_one_map().cpu().numpy(), orc.one_one_map(N, M, IF))
+    mo, so = orc.one_two_map(N, M, IF)
+    m, s = sp.two_map(False)
+    assert np.array_equal(m.cpu().numpy(), mo) and np.array_equal(s.cpu().numpy(), so)
+    mo, so = orc.two_two_map(N, M, IF)
+    m, s = sp.two_map(True)
+    assert np.array_equal(m.cpu().numpy(), mo) and np.array_equal(s.cpu().numpy(), so)
+
+
+# ----------------------------------------------------------------- H.psi ----
+
+def test_hpsi_golden(golden_ops):
+    for kind, N, M in case_keys(golden_ops, "hxx"):
+        key = f"{kind}_{N}_{M}"
+        C, Ho, Hint = golden_ops[f"C_{key}"], golden_ops[f"Ho_{key}"], golden_ops[f"Hint_{key}"]
+        sp = _space(N, M)
+        sp.set_integrals(Ho, Hint, mc.VARIANT_MAPS)
+        assert rel(sp.apply_h(C).cpu().numpy(), golden_ops[f"hxx_{key}"]) <= TOL, key
+        sp.set_integrals(Ho, Hint, mc.VARIANT_HASH)
+        assert rel(sp.apply_h(C).cpu().numpy(), golden_ops[f"hplain_{key}"]) <= TOL, key
+        sp.close()
+
+
+@pytest.mark.parametrize("N,M,seed", [(10, 10, 0), (6, 8, 1), (9, 5, 2), (4, 16, 3), (12, 4, 4)])
+def test_hpsi_random_oracle(orc, N, M, seed):
+    C, Ho, Hint = mc.random_problem(N, M, seed)
+    sp = _space(N, M)
+    sp.set_integrals(Ho, Hint)
+    out = sp.apply_h(C).cpu().numpy()
+    assert rel(out, orc.apply_h(N, M, C, Ho, Hint, mode=2)) <= TOL
+
+
+@pytest.mark.parametrize("N,M", [(6, 5), (5, 7)])
+def test_hpsi_unsymmetric_hint_follows_each_variant(orc, N, M):
+    # Without the 8-fold symmetry the reference variants disagree with each
+    # other; the device path must reproduce whichever one it is asked for.
+    rng = np.random.default_rng(11)
+    C, Ho, _ = mc.random_problem(N, M, 5)
+    Ho = Ho + 0.2j * rng.standard_normal((M, M))            # not Hermitian either
+    Hint = rng.standard_normal(M ** 4) + 1j * rng.standard_normal(M ** 4)
+    sp = _space(N, M)
+    sp.set_integrals(Ho, Hint, mc.VARIANT_MAPS)
+    assert rel(sp.apply_h(C).cpu().numpy(), orc.apply_h(N, M, C, Ho, Hint, mode=2)) <= TOL
+    sp.set_integrals(Ho, Hint, mc.VARIANT_HASH)
+    assert rel(sp.apply_h(C).cpu().numpy(), orc.apply_h(N, M, C, Ho, Hint, mode=0)) <= TOL
+
+
+@pytest.mark.parametrize("N,M", [(0, 4), (1, 1), (1, 6), (2, 1), (2, 5), (3, 2), (7, 1), (5, 16)])
+def test_hpsi_edge_sizes(orc, N, M):
+    C, Ho, Hint = mc.random_problem(N, M, 9)
+    sp = _space(N, M)
+    sp.set_integrals(Ho, Hint)
+    out = sp.apply_h(C).cpu().numpy()
+    ref = orc.apply_h(N, M, C, Ho, Hint, mode=2)
+    assert rel(out, ref) <= TOL, (N, M)
+
+
+def test_hpsi_lieb(orc):
+    N, M = 8, 9
+    Ho, Hint = mc.lieb_integrals(M, 2.5)
+    C = orc.perf_inputs(N, M)[0]
+    sp = _space(N, M)
+    sp.set_integrals(Ho, Hint)
+    assert rel(sp.apply_h(C).cpu().numpy(), orc.apply_h(N, M, C, Ho, Hint, mode=2)) <= TOL
+
+
+def test_adjoint():
+    N, M = 6, 6
+    rng = np.random.default_rng(2)
+    C, Ho, Hint = mc.random_problem(N, M, 3)
+    Hint = Hint + 0.1 * (rng.standard_normal(M ** 4) + 1j * rng.standard_normal(M ** 4))
+    Ho = Ho + 0.1j * rng.standard_normal((M, M))
+    phi = mc.random_problem(N, M, 4)[0]
+    sp = _space(N, M)
+    sp.set_integrals(Ho, Hint)
+    lhs = np.vdot(phi, sp.apply_h(C).cpu().numpy())
+    rhs = np.vdot(sp.apply_h_adjoint(phi).cpu().numpy(), C)
+    assert abs(lhs - rhs) <= 1e-12 * abs(lhs)
+
+
+# ------------------------------------------------------------- densities ----
+
+def test_densities_golden(golden_ops):
+    for kind, N, M in case_keys(golden_ops, "rho1"):
+        key = f"{kind}_{N}_{M}"
+        C = golden_ops[f"C_{key}"]
+        sp = _space(N, M)
+        assert rel(sp.rho1(C).cpu().numpy(), golden_ops[f"rho1_{key}"]) <= TOL, key
+        assert rel(sp.rho2(C).cpu().numpy(), golden_ops[f"rho2_{key}"]) <= TOL, key
+        sp.close()
+
+
+@pytest.mark.parametrize("N,M", [(10, 10), (7, 11), (3, 16), (1, 5), (0, 3)])
+def test_densities_oracle(orc, N, M):
+    C = mc.random_problem(N, M, 21)[0]
+    sp = _space(N, M)
+    r1 = sp.rho1(C).cpu().numpy()
+    assert rel(r1, orc.obrho(N, M, C)) <= TOL
+    assert abs(np.trace(r1) - N) <= 1e-12 * max(N, 1)
+    r2 = sp.rho2(C).cpu().numpy()
+    if N * M ** 4 * orc.nc(N, M) <= 2e9:
+        assert rel(r2, orc.density(N, M, 2, C, C)) <= TOL
+    R = r2.reshape(M, M, M, M)          # axes (l, q, s, k)
+    tr = sum(R[k, s, s, k] for k in range(M) for s in range(M))   # sum <a+_k a+_s a_s a_k>
+    assert abs(tr - N * (N - 1)) <= 1e-12 * max(1, N * N)
+
+
+@pytest.mark.parametrize("N,M", [(5, 5), (6, 7), (2, 4)])
+def test_transition_densities(orc, N, M):
+    phi = mc.random_problem(N, M, 31)[0]
+    psi = mc.random_problem(N, M, 32)[0]
+    sp = _space(N, M)
+    t1 = sp.trans_rho1(phi, psi).cpu().numpy()
+    o1 = orc.density(N, M, 1, phi, psi).reshape(M, M).T      # oracle flat k + l*M
+    assert rel(t1, o1) <= TOL
+    t2 = sp.trans_rho2(phi, psi).cpu().numpy()
+    assert rel(t2, orc.density(N, M, 2, phi, psi)) <= TOL
+
+
+def test_energy_identity_device():
+    N, M = 7, 8
+    C, Ho, Hint = mc.random_problem(N, M, 41)
+    sp = _space(N, M)
+    sp.set_integrals(Ho, Hint)
+    e1 = np.vdot(C, sp.apply_h(C).cpu().numpy())
+    e2 = np.sum(Ho * sp.rho1(C).cpu().numpy()) + 0.5 * np.sum(Hint * sp.rho2(C).cpu().numpy())
+    assert abs(e1 - e2) <= 1e-12 * abs(e1)
+
+
+# ---------------------------------------------------------------- Lanczos ----
+
+def test_lanczos_coefficients(orc):
+    N, M, lm = 6, 6, 30
+    Ho, Hint = mc.lieb_integrals(M, 4.0)
+    C0 = orc.perf_inputs(N, M)[0]
+    sp = _space(N, M)
+    sp.set_integrals(Ho, Hint)
+    it, diag, off, _ = sp.lanczos(C0, lm)
+    ito, diago, offo, _ = orc.lanczos(N, M, Ho, Hint, C0, lm, mode=2)
+    assert it == ito == lm
+    scale = np.abs(diago).max()
+    assert np.abs(diag[:it] - diago[:it]).max() <= 1e-10 * scale
+    assert np.abs(off[: it - 1] - offo[: it - 1].real).max() <= 1e-10 * scale
+
+
+def test_ground_lieb_known_answers(orc, golden_lieb):
+    N, M, niter = int(golden_lieb["N"]), int(golden_lieb["M"]), int(golden_lieb["niter"])
+    C0 = orc.perf_inputs(N, M)[0]
+    pub = dict(zip(golden_lieb["published_g"], golden_lieb["published_E0_per_N"]))
+    sp = _space(N, M)
+    for g, Eref in zip(golden_lieb["g"], golden_lieb["E0"]):
+        Ho, Hint = mc.lieb_integrals(M, g)
+        sp.set_integrals(Ho, Hint)
+        E, psi, it = sp.ground(C0, niter)
+        assert it == niter
+        assert abs(E - Eref) <= 1e-10 * max(1.0, abs(Eref)), (g, E, Eref)
+        assert round(E / N, 5) == pytest.approx(pub[g], abs=1e-5)
+        # the Ritz vector is an eigenvector
+        hpsi = sp.apply_h(psi)
+        res = torch.linalg.vector_norm(hpsi - E * psi).item() / torch.linalg.vector_norm(psi).item()
+        assert res < 1e-6 * abs(E)
+
+
+def test_ground_random_against_oracle(orc):
+    N, M, niter = 7, 6, 60
+    C0, Ho, Hint = mc.random_problem(N, M, 51)
+    sp = _space(N, M)
+    sp.set_integrals(Ho, Hint)
+    E, psi, it = sp.ground(C0, niter)
+    Eo, psio, ito = orc.ground(N, M, Ho, Hint, C0, niter, mode=2)
+    assert it == ito
+    assert abs(E - Eo) <= 1e-10 * max(1.0, abs(Eo))
+    ov = abs(np.vdot(psi.cpu().numpy(), psio)) / (np.linalg.norm(psio) ** 2)
+    assert abs(ov - 1) < 1e-8
+
+
+def test_lanczos_breakdown():
+    # all particles in one plane wave of a non-interacting ring: the start
+    # vector is an eigenvector, beta_0 = 0 and the solve stops at once
+    N, M = 4, 5
+    Ho, Hint = mc.lieb_integrals(M, 0.0)
+    C0 = np.zeros(mc.nc_of(N, M), np.complex128)
+    C0[mc.FockToIndex(N, M, [0, 0, 4, 0, 0])] = 1.0
+    sp = _space(N, M)
+    sp.set_integrals(Ho, Hint)
+    it, diag, off, _ = sp.lanczos(C0, 10)
+    assert it == 0
+    E, psi, it2 = sp.ground(C0, 10)
+    assert it2 == 0 and E == pytest.approx(diag[0].real)
