@@ -1,0 +1,377 @@
+#!/usr/bin/env python
+"""Benchmark of the mcpi hot path on B200.
+
+Workload (N=1): the Lieb-Liniger gas of N=16 bosons in M=10 plane waves on a
+ring of length L=1, g=1.0 (dimension 2,042,975; integrals of
+groundStateLieb.c:129-213), seeded synthetic complex-normal states.
+
+A step is one H.psi of that configuration; `value` is whole-job H.psi/s with
+the states resident in HBM, eight distinct states rotating between steps
+(8 x 32.7 MB > the 126 MB L2, so every step reads a state that is not cached).
+`e2e` is the same metric through the public API with the state copied from
+pinned host memory and the result copied back inside every step. The line
+also carries the roofline of the dominant kernel (CUDA events, measured live),
+a 150-step Lanczos ground-state solve of the same configuration, and the CPU
+baseline: the oracle's restatement of the reference's applyHconf_X
+(hamiltonianMatrix.h:431-887; the reference's fastest CPU H.psi that runs at
+this size) on a bounded row sample with all host threads.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mcpi|reference]
+
+With --gpus N > 1 (under torchrun) each rank runs an independent replica of
+the workload on its own GPU (the solve does not shard: weak scaling).
+`--impl reference` times the CPU oracle port alone (rank 0), on the same
+config, metric and unit.
+"""
+import argparse
+import json
+import os
+import re
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "H·ψ/s (HBM GB/s) & batched E0 solves/s vs plain GPU path at |ΔE0|≤1e-10"
+UNIT = "H·ψ/s"
+N_PART, M_ORB, G, L_RING = 16, 10, 1.0, 1.0
+ROTATE = 8
+LANCZOS_ITERS = 150
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=2000)
+    p.add_argument("--warmup", type=int, default=10)
+    p.add_argument("--impl", default="mcpi", choices=["mcpi", "reference"])
+    p.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-lanczos", action="store_true")
+    return p.parse_args()
+
+
+def config(extra=None):
+    c = {"workload": "Lieb-Liniger N=16 M=10 g=1 L=1, H.psi (nc=2042975)",
+         "N": N_PART, "M": M_ORB, "g": G, "nc": 2042975,
+         "l2": f"{ROTATE} rotating states of 32.7 MB (> 126 MB L2)",
+         "parallelism": "replicas"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+# ---------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+
+    def start(self):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-i", str(self.device), "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.f.flush()
+        rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = max(mx, float(r[2]))
+                for nm, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# roofline inputs
+# ---------------------------------------------------------------------------
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, or None."""
+    p = os.path.join(ROOT, "profiles", "hpsi_lieb_n16_m10.md")
+    if not os.path.exists(p):
+        return None
+    m = re.search(rf"^traffic_bytes_per_launch\s+{kernel}\s+([0-9.eE+]+)", open(p).read(), re.M)
+    return float(m.group(1)) if m else None
+
+
+def hpsi_bytes(nc, nc2, P):
+    """Algorithmic HBM bytes per launch of the two H.psi kernels: kernel 1
+    reads psi once and writes the P x nc2 intermediate E; kernel 2 reads E and
+    psi and writes out (16 B per complex)."""
+    return {"pair_annihilate": 16 * nc + 16 * P * nc2, "pair_create": 16 * P * nc2 + 32 * nc}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: oracle restatement of applyHconf_X on a row sample
+# ---------------------------------------------------------------------------
+
+def cpu_setup(N, M, g):
+    import oracle
+    O = oracle.Orc()
+    IF = O.focks(N, M)
+    Map = O.one_one_map(N, M, IF)
+    MapOT, sOT = O.one_two_map(N, M, IF)
+    Ho, Hint = O.lieb(M, g, L_RING)
+    C = np.random.default_rng(5).standard_normal(O.nc(N, M)) + 0j
+    return O, IF, (Map, MapOT, sOT, None, None), Ho, Hint, C
+
+
+def cpu_rows(O, st, row0, nrows, threads, out):
+    IF, maps, Ho, Hint, C = st
+    nc = O.nc(N_PART, M_ORB)
+    O.apply_h(N_PART, M_ORB, C, Ho, Hint, mode=1, IF=IF, maps=maps, row0=row0,
+              row1=min(nc, row0 + nrows), threads=threads, out=out)
+
+
+def cpu_baseline(budget_s):
+    threads = len(os.sched_getaffinity(0))
+    O, IF, maps, Ho, Hint, C = cpu_setup(N_PART, M_ORB, G)
+    st = (IF, maps, Ho, Hint, C)
+    nc = O.nc(N_PART, M_ORB)
+    out = np.zeros(nc, np.complex128)
+    # calibrate on a strided sample of 16 chunks spread over the index range
+    chunks = 16
+    rows = 256
+    while True:
+        t0 = time.perf_counter()
+        for c in range(chunks):
+            cpu_rows(O, st, c * (nc // chunks), rows, threads, out)
+        dt = time.perf_counter() - t0
+        if dt > budget_s / 8 or rows * chunks >= nc:
+            break
+        rows *= 2
+    target = int(rows * budget_s / max(dt, 1e-6))
+    rows = max(1, min(nc // chunks, target))
+    t0 = time.perf_counter()
+    for c in range(chunks):
+        cpu_rows(O, st, c * (nc // chunks), rows, threads, out)
+    dt = time.perf_counter() - t0
+    sampled = rows * chunks
+    return {"value": (sampled / nc) / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{sampled} of {nc} rows ({chunks} chunks spread over the index range) of "
+                      f"the applyHconf_X restatement (oracle/mcpi_oracle.c), {dt:.1f} s, "
+                      f"OpenMP over rows; value = sampled fraction / time",
+            "seconds": dt}
+
+
+# ---------------------------------------------------------------------------
+# reference arm
+# ---------------------------------------------------------------------------
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    threads = len(os.sched_getaffinity(0))
+    O, IF, maps, Ho, Hint, C = cpu_setup(N_PART, M_ORB, G)
+    st = (IF, maps, Ho, Hint, C)
+    nc = O.nc(N_PART, M_ORB)
+    out = np.zeros(nc, np.complex128)
+    # size each step so that warm-up + steps stay within ~2 minutes
+    t0 = time.perf_counter()
+    cpu_rows(O, st, nc // 3, 2048, threads, out)
+    per_row = (time.perf_counter() - t0) / 2048
+    rows = int(max(64, min(nc, 120.0 / max(1, args.steps + args.warmup) / per_row)))
+    starts = np.linspace(0, nc - rows, 97).astype(np.int64)
+    for w in range(args.warmup):
+        cpu_rows(O, st, int(starts[w % len(starts)]), rows, threads, out)
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        cpu_rows(O, st, int(starts[k % len(starts)]), rows, threads, out)
+    dt = time.perf_counter() - t0
+    value = args.steps * (rows / nc) / dt
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+            "data": "synthetic", "impl": "reference",
+            "config": config({"parallelism": "cpu", "rows_per_step": rows}),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{rows} rows per step of the applyHconf_X restatement "
+                                       f"(oracle/mcpi_oracle.c), steps rotate over 97 offsets"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# mcpi arm
+# ---------------------------------------------------------------------------
+
+def run_mcpi(args):
+    import torch
+    import torch.distributed as dist
+
+    import mcpi_b200 as mc
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    N, M = N_PART, M_ORB
+    sp = mc.FockSpace(N, M, device=local)
+    Ho, Hint = mc.lieb_integrals(M, G, L_RING)
+    sp.set_integrals(Ho, Hint)
+    nc, P, nc2 = sp.nc, sp.P, mc.nc_of(N - 2, M)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(1234 + rank)
+    X = torch.randn((ROTATE, nc), dtype=torch.complex128, device=dev, generator=gen)
+    X /= torch.linalg.vector_norm(X, dim=1, keepdim=True)
+    out = torch.empty(nc, dtype=torch.complex128, device=dev)
+
+    # ---- device-resident H.psi ----
+    for w in range(args.warmup):
+        sp.apply_h(X[w % ROTATE], out)
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for k in range(args.steps):
+        sp.apply_h(X[k % ROTATE], out)
+    e1.record()
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    value = world * args.steps / (ms / 1e3)
+
+    # ---- roofline of the dominant kernel (CUDA events on the launching stream) ----
+    k1, k2 = sp.apply_h_profile(X[0], out, reps=20)
+    names = ["pair_annihilate", "pair_create"]
+    times = {"pair_annihilate": k1, "pair_create": k2}
+    dom = max(names, key=lambda n: times[n])
+    byts = hpsi_bytes(nc, nc2, P)
+    peak, peak_kind = measured_peak()
+    achieved = byts[dom] / (times[dom] * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_source": peak_kind,
+                "traffic": ncu_traffic(dom), "algorithmic_bytes": byts[dom],
+                "kernel_ms": {n: times[n] for n in names},
+                "hpsi_achieved_gbs": (byts["pair_annihilate"] + byts["pair_create"]) / (ms / args.steps * 1e-3) / 1e9}
+
+    # ---- e2e through the public API with pinned host buffers ----
+    hx = torch.empty(nc, dtype=torch.complex128).pin_memory()
+    hx.copy_(X[0].cpu())
+    ho = torch.empty(nc, dtype=torch.complex128).pin_memory()
+    dx = torch.empty(nc, dtype=torch.complex128, device=dev)
+    ke = max(10, min(args.steps, 200))
+    for w in range(3):
+        dx.copy_(hx, non_blocking=True)
+        sp.apply_h(dx, out)
+        ho.copy_(out, non_blocking=True)
+    torch.cuda.synchronize()
+    barrier()
+    a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a0.record()
+    for k in range(ke):
+        dx.copy_(hx, non_blocking=True)
+        sp.apply_h(dx, out)
+        ho.copy_(out, non_blocking=True)
+    a1.record()
+    torch.cuda.synchronize()
+    barrier()
+    ems = max_over_ranks(a0.elapsed_time(a1))
+    e2e = {"value": world * ke / (ems / 1e3), "unit": UNIT, "h2d_bytes_per_step": 16 * nc,
+           "d2h_bytes_per_step": 16 * nc, "steps": ke}
+
+    # ---- Lanczos ground state of the same configuration ----
+    lanczos = None
+    if not args.no_lanczos:
+        C0 = X[0].clone()
+        torch.cuda.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        E0, psi, it = sp.ground(C0, LANCZOS_ITERS)
+        dt = max_over_ranks(time.perf_counter() - t0)
+        occ = sp.rho1(psi).diagonal().real.cpu().numpy()
+        lanczos = {"iterations": it, "E0": E0, "E0_per_N": E0 / N, "seconds": dt,
+                   "solves_per_s": world / dt, "occupations": [round(float(o), 6) for o in occ]}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args.cpu_seconds)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+                "config": config(), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": 2 * args.steps, "clocks": clk, "lanczos": lanczos}
+        print(json.dumps(line), flush=True)
+    sp.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_mcpi(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -37,6 +37,7 @@ extern "C" {
 #define MCPI_ERR_NOMEM 4        /* device or host allocation failed */
 #define MCPI_ERR_STATE 5        /* call order (e.g. no integrals set) */
 #define MCPI_ERR_NUMERIC 6      /* tridiagonal eigensolver did not converge */
+#define MCPI_ERR_TIMEOUT 7      /* a kernel's bounded wait expired (its output is invalid) */
 
 /* variants of the two-body folding (see mcpi_set_integrals) */
 #define MCPI_VARIANT_MAPS 0     /* applyHconf_X / _XX / _omp and the CUDA kernel */
@@ -58,6 +59,19 @@ MCPI_API int mcpi_space_destroy(mcpi_space sp);
  * legacy default stream). A new space uses a private non-blocking stream. */
 MCPI_API int mcpi_space_set_stream(mcpi_space sp, void *stream);
 MCPI_API int mcpi_space_sync(mcpi_space sp);
+/* Space options. MCPI_OPT_DENSE_PAIR_KERNEL (value 0/1): always use the dense
+ * pair-matrix kernel for H.psi even when the integrals decompose into small
+ * blocks (takes effect at the next mcpi_set_integrals). */
+#define MCPI_OPT_DENSE_PAIR_KERNEL 1
+/* MCPI_OPT_NO_MOMENTUM_KERNEL (0/1): do not use the momentum-block kernel
+ * (chosen when the pair matrix only couples pairs of equal total orbital index,
+ * as plane-wave integrals of a translation-invariant interaction do). */
+#define MCPI_OPT_NO_MOMENTUM_KERNEL 2
+/* MCPI_OPT_CREATE_FORM: form of the pair-creation kernel of H.psi -- 0 per-row
+ * tables in shared memory (default), 1 per-row tables in registers. Takes
+ * effect at the next mcpi_set_integrals. */
+#define MCPI_OPT_CREATE_FORM 3
+MCPI_API int mcpi_space_set_option(mcpi_space sp, int option, int value);
 MCPI_API int mcpi_space_dims(mcpi_space sp, int *N, int *M, int64_t *nc);
 
 /* ---- tables in the reference layouts, built on the device ---------------- */
@@ -87,6 +101,11 @@ MCPI_API int mcpi_set_integrals(mcpi_space sp, const double *h_Ho, const double 
 /* out = H C (hamiltonianMatrix.h:891-1425 applyHconf_XX semantics; _omp, _X and
  * the CUDA applyHconf kernel compute the same; MCPI_VARIANT_HASH gives applyHconf). */
 MCPI_API int mcpi_apply_h(mcpi_space sp, const void *d_C, void *d_out);
+/* mcpi_apply_h, timed: runs it reps times with CUDA events around each of its
+ * two kernels on the space's stream (synchronising after every repetition) and
+ * returns their mean durations in ms: h_ms[0] pair annihilation + pair-matrix
+ * kernel, h_ms[1] pair creation kernel. For measurement, not for production. */
+MCPI_API int mcpi_apply_h_profile(mcpi_space sp, const void *d_C, void *d_out, int reps, float *h_ms);
 /* out = H^dagger C (adjoint of the operator above; equal to H C when Ho is
  * Hermitian and Hint has the 8-fold symmetry). No reference counterpart. */
 MCPI_API int mcpi_apply_h_adjoint(mcpi_space sp, const void *d_C, void *d_out);

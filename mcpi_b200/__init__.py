@@ -63,6 +63,7 @@ def lib():
         "mcpi_space_destroy": (i, [_vp]),
         "mcpi_space_set_stream": (i, [_vp, _vp]),
         "mcpi_space_sync": (i, [_vp]),
+        "mcpi_space_set_option": (i, [_vp, i, i]),
         "mcpi_space_dims": (i, [_vp, pi, pi, p64]),
         "mcpi_ncmat": (i, [i, i, _vp]),
         "mcpi_index_to_fock": (i, [i, i, i64, _vp]),
@@ -74,6 +75,7 @@ def lib():
         "mcpi_set_integrals": (i, [_vp, _vp, _vp, i]),
         "mcpi_apply_h": (i, [_vp, _vp, _vp]),
         "mcpi_apply_h_adjoint": (i, [_vp, _vp, _vp]),
+        "mcpi_apply_h_profile": (i, [_vp, _vp, _vp, i, _vp]),
         "mcpi_rho1": (i, [_vp, _vp, _vp]),
         "mcpi_rho2": (i, [_vp, _vp, _vp]),
         "mcpi_trans_rho1": (i, [_vp, _vp, _vp, _vp]),
@@ -218,6 +220,17 @@ class FockSpace:
     def sync(self):
         _check(lib().mcpi_space_sync(self._h))
 
+    def set_dense_pair_kernel(self, on: bool = True):
+        """Force the dense pair-matrix H.psi kernel (applies at the next set_integrals)."""
+        _check(lib().mcpi_space_set_option(self._h, 1, int(on)))
+
+    def set_option(self, option: int, value: int):
+        _check(lib().mcpi_space_set_option(self._h, int(option), int(value)))
+
+    def set_momentum_kernel(self, on: bool = True):
+        """Allow (default) or forbid the momentum-block H.psi kernel (next set_integrals)."""
+        _check(lib().mcpi_space_set_option(self._h, 2, int(not on)))
+
     # tables ----------------------------------------------------------------
     def focks(self):
         """IF[j + i*M] (configurationsMap.h:309-344), int32 tensor."""
@@ -263,6 +276,16 @@ class FockSpace:
         self._stream()
         _check(lib().mcpi_apply_h(self._h, _vp(C.data_ptr()), _vp(out.data_ptr())))
         return out
+
+    def apply_h_profile(self, C, out=None, reps: int = 10):
+        """Mean CUDA-event durations (ms) of the two H.psi kernels."""
+        C = self._vec(C)
+        out = self.empty() if out is None else out
+        ms = np.zeros(2, np.float32)
+        self._stream()
+        _check(lib().mcpi_apply_h_profile(self._h, _vp(C.data_ptr()), _vp(out.data_ptr()), reps,
+                                          _np_ptr(ms)))
+        return float(ms[0]), float(ms[1])
 
     def apply_h_adjoint(self, C, out=None):
         C = self._vec(C)

@@ -90,7 +90,14 @@ struct DevPairOp {
     double2 *hdiag = nullptr;
     double2 *hfull = nullptr;
     int nnz = 0;
-    PairOp view() const { return PairOp{rowptr, col, val, hdiag, hfull, nnz}; }
+    int *prog = nullptr;       // block-sparse form (nullptr when a block is too wide)
+    int prog_bytes = 0;
+    double2 *hblk = nullptr;   // momentum-block form (nullptr when Ht couples different q+l)
+    int nhblk = 0;
+    int create_form = 0;
+    int *status = nullptr;     // the space's device status word (not owned)
+    PairOp view() const { return PairOp{rowptr, col, val, hdiag, hfull, nnz, hblk, nhblk, create_form, status}; }
+    mcpi::BlockOp blocks() const { return mcpi::BlockOp{prog, prog_bytes}; }
 };
 
 }  // namespace
@@ -109,6 +116,10 @@ struct mcpi_space_s {
     double2 *d_gram = nullptr;       // density partials
     size_t gram_cap = 0;
     double2 *d_dot = nullptr;        // 1 result + partials
+    int *d_status = nullptr;         // device status word: 1 = a kernel's bounded wait timed out
+    bool dense_only = false;         // force the dense pair-matrix kernel
+    int kernel_choice = 0;           // 2: skip the momentum-block kernel
+    int create_form = 0;            // pair-creation kernel form (MCPI_OPT_CREATE_FORM)
     SpaceTables tables() const { return SpaceTables{d_W, d_sq}; }
 };
 
@@ -116,6 +127,8 @@ namespace {
 
 void free_op(DevPairOp &o)
 {
+    cudaFree(o.hblk);
+    cudaFree(o.prog);
     cudaFree(o.rowptr);
     cudaFree(o.col);
     cudaFree(o.val);
@@ -184,6 +197,84 @@ std::vector<cplx> build_pair_matrix(int N, int M, const cplx *Ho, const cplx *Hi
     return Ht;
 }
 
+// Decomposes Ht into independent blocks (connected components of the
+// bipartite row/column graph of its nonzeros) and packs them for the
+// block-sparse kernel (layout in kernels.h, BlockOp). Empty vector when some
+// block has more than kBlockCols columns or the packed form is too large.
+std::vector<int> pack_blocks(const std::vector<cplx> &Ht, int P, int M)
+{
+    std::vector<int> parent(2 * P);
+    for (int x = 0; x < 2 * P; ++x) parent[x] = x;
+    auto find = [&](int x) {
+        while (parent[x] != x) x = parent[x] = parent[parent[x]];
+        return x;
+    };
+    for (int a = 0; a < P; ++a)
+        for (int b = 0; b < P; ++b)
+            if (Ht[(size_t)a * P + b] != cplx(0.0, 0.0)) parent[find(a)] = find(P + b);
+    std::vector<std::vector<int>> brow(2 * P), bcol(2 * P);
+    for (int a = 0; a < P; ++a) brow[find(a)].push_back(a);
+    for (int b = 0; b < P; ++b) bcol[find(P + b)].push_back(b);
+    std::vector<int> roots;
+    for (int x = 0; x < 2 * P; ++x)
+        if (!brow[x].empty()) {
+            if ((int)bcol[x].size() > mcpi::kBlockCols) return {};
+            roots.push_back(x);
+        }
+    std::vector<int> qs(P), ls(P);
+    for (int q = 0; q < M; ++q)
+        for (int l = q; l < M; ++l) {
+            qs[mcpi::pair_index(q, l, M)] = q;
+            ls[mcpi::pair_index(q, l, M)] = l;
+        }
+    const int nb = (int)roots.size();
+    std::vector<int> hdr, cols, rows;
+    std::vector<cplx> vals;
+    for (int x : roots) {
+        hdr.push_back((int)cols.size());
+        hdr.push_back((int)bcol[x].size());
+        hdr.push_back((int)rows.size());
+        hdr.push_back((int)brow[x].size());
+        hdr.push_back((int)vals.size());
+        for (int b : bcol[x]) cols.push_back(qs[b] | (ls[b] << 8));
+        for (int a : brow[x]) {
+            rows.push_back(a);
+            for (int b : bcol[x]) vals.push_back(Ht[(size_t)a * P + b]);
+        }
+    }
+    std::vector<int> prog = {nb, (int)cols.size(), (int)rows.size(), (int)vals.size()};
+    prog.insert(prog.end(), hdr.begin(), hdr.end());
+    prog.insert(prog.end(), cols.begin(), cols.end());
+    prog.insert(prog.end(), rows.begin(), rows.end());
+    while ((prog.size() * 4) % 16) prog.push_back(0);
+    const size_t off = prog.size();
+    prog.resize(off + vals.size() * 4);
+    std::memcpy(prog.data() + off, vals.data(), vals.size() * sizeof(cplx));
+    if (prog.size() * 4 > 96 * 1024) return {};
+    return prog;
+}
+
+// Momentum-block packing (layout in kernels.h, PairOp::hblk): empty when Ht
+// couples two pairs of different total q + l.
+std::vector<cplx> pack_momentum(const std::vector<cplx> &Ht, int P, int M)
+{
+    for (int k = 0; k < M; ++k)
+        for (int s = k; s < M; ++s)
+            for (int q = 0; q < M; ++q)
+                for (int l = q; l < M; ++l)
+                    if (k + s != q + l &&
+                        Ht[(size_t)mcpi::pair_index(k, s, M) * P + mcpi::pair_index(q, l, M)] != cplx(0.0, 0.0))
+                        return {};
+    std::vector<cplx> out;
+    for (int K = 0; K <= 2 * M - 2; ++K) {
+        const int qlo = K - (M - 1) > 0 ? K - (M - 1) : 0, qhi = K / 2;
+        for (int r = qlo; r <= qhi; ++r)
+            for (int c = qlo; c <= qhi; ++c)
+                out.push_back(Ht[(size_t)mcpi::pair_index(r, K - r, M) * P + mcpi::pair_index(c, K - c, M)]);
+    }
+    return out;
+}
+
 int upload_op(mcpi_space_s *sp, DevPairOp &op, const std::vector<cplx> &Ht, const cplx *hdiag,
               const cplx *hfull)
 {
@@ -215,6 +306,18 @@ int upload_op(mcpi_space_s *sp, DevPairOp &op, const std::vector<cplx> &Ht, cons
     }
     CK(cudaMemcpyAsync(op.hdiag, hdiag, sizeof(double2) * M, cudaMemcpyHostToDevice, sp->stream));
     CK(cudaMemcpyAsync(op.hfull, hfull, sizeof(double2) * M * M, cudaMemcpyHostToDevice, sp->stream));
+    const std::vector<cplx> mom = pack_momentum(Ht, P, M);
+    if (!mom.empty() && !sp->dense_only && sp->kernel_choice != 2) {
+        CK(cudaMalloc(&op.hblk, sizeof(double2) * mom.size()));
+        CK(cudaMemcpyAsync(op.hblk, mom.data(), sizeof(double2) * mom.size(), cudaMemcpyHostToDevice, sp->stream));
+        op.nhblk = (int)mom.size();
+    }
+    const std::vector<int> prog = pack_blocks(Ht, P, M);
+    if (!prog.empty() && !sp->dense_only) {
+        CK(cudaMalloc(&op.prog, sizeof(int) * prog.size()));
+        CK(cudaMemcpyAsync(op.prog, prog.data(), sizeof(int) * prog.size(), cudaMemcpyHostToDevice, sp->stream));
+        op.prog_bytes = (int)(sizeof(int) * prog.size());
+    }
     CK(cudaStreamSynchronize(sp->stream));  // host vectors go out of scope
     op.nnz = (int)col.size();
     return MCPI_OK;
@@ -248,8 +351,8 @@ int apply_op(mcpi_space_s *sp, const DevPairOp &op, const void *d_C, void *d_out
     DeviceGuard g(sp->device);
     int rc = ensure_E(sp);
     if (rc) return rc;
-    CK(mcpi::launch_apply_h(sp->sp, sp->tables(), op.view(), (const double2 *)d_C, sp->d_E,
-                            (double2 *)d_out, sp->stream));
+    CK(mcpi::launch_apply_h(sp->sp, sp->tables(), op.view(), op.blocks(), (const double2 *)d_C,
+                            sp->d_E, (double2 *)d_out, sp->stream));
     return MCPI_OK;
 }
 
@@ -267,6 +370,7 @@ const char *mcpi_status_string(int status)
     case MCPI_ERR_NOMEM: return "out of memory";
     case MCPI_ERR_STATE: return "invalid call order";
     case MCPI_ERR_NUMERIC: return "numerical failure";
+    case MCPI_ERR_TIMEOUT: return "device wait timed out";
     default: return "unknown status";
     }
 }
@@ -328,6 +432,8 @@ int mcpi_space_create(int N, int M, int device, mcpi_space *out)
     if (e == cudaSuccess) e = cudaMalloc(&s->d_W, sizeof(uint32_t) * W.size());
     if (e == cudaSuccess) e = cudaMalloc(&s->d_sq, sizeof(double) * ws);
     if (e == cudaSuccess) e = cudaMalloc(&s->d_dot, sizeof(double2) * (mcpi::lanczos_parts(nc) + 1));
+    if (e == cudaSuccess) e = cudaMalloc(&s->d_status, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(s->d_status, 0, sizeof(int));
     if (e == cudaSuccess) e = cudaMemcpy(s->d_W, W.data(), sizeof(uint32_t) * W.size(), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(s->d_sq, sq.data(), sizeof(double) * ws, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
@@ -352,6 +458,7 @@ int mcpi_space_destroy(mcpi_space sp)
     cudaFree(sp->d_E);
     cudaFree(sp->d_gram);
     cudaFree(sp->d_dot);
+    cudaFree(sp->d_status);
     if (sp->own) cudaStreamDestroy(sp->own);
     delete sp;
     return MCPI_OK;
@@ -364,12 +471,39 @@ int mcpi_space_set_stream(mcpi_space sp, void *stream)
     return MCPI_OK;
 }
 
+int mcpi_space_set_option(mcpi_space sp, int option, int value)
+{
+    CHECK_ARG(sp, "null space");
+    switch (option) {
+    case MCPI_OPT_DENSE_PAIR_KERNEL: sp->dense_only = value != 0; return MCPI_OK;
+    case MCPI_OPT_NO_MOMENTUM_KERNEL: sp->kernel_choice = value ? 2 : 0; return MCPI_OK;
+    case MCPI_OPT_CREATE_FORM:
+        sp->create_form = value;
+        sp->fwd.create_form = sp->adj.create_form = value;
+        return MCPI_OK;
+    default: return fail(MCPI_ERR_ARG, "unknown option %d", option);
+    }
+}
+
+// Reads and clears the device status word (after a stream synchronisation).
+static int check_status(mcpi_space_s *sp)
+{
+    int st = 0;
+    CK(cudaMemcpyAsync(&st, sp->d_status, sizeof(int), cudaMemcpyDeviceToHost, sp->stream));
+    CK(cudaStreamSynchronize(sp->stream));
+    if (st) {
+        CK(cudaMemsetAsync(sp->d_status, 0, sizeof(int), sp->stream));
+        return fail(MCPI_ERR_TIMEOUT, "a device-side bounded wait timed out (status %d)", st);
+    }
+    return MCPI_OK;
+}
+
 int mcpi_space_sync(mcpi_space sp)
 {
     CHECK_ARG(sp, "null space");
     DeviceGuard g(sp->device);
     CK(cudaStreamSynchronize(sp->stream));
-    return MCPI_OK;
+    return check_status(sp);
 }
 
 int mcpi_space_dims(mcpi_space sp, int *N, int *M, int64_t *nc)
@@ -529,11 +663,48 @@ int mcpi_set_integrals(mcpi_space sp, const double *h_Ho, const double *h_Hint, 
     if (rc) return rc;
     rc = upload_op(sp, sp->adj, Hta, hda.data(), hfa.data());
     if (rc) return rc;
+    sp->fwd.create_form = sp->adj.create_form = sp->create_form;
+    sp->fwd.status = sp->adj.status = sp->d_status;
     sp->has_op = true;
     return MCPI_OK;
 }
 
 int mcpi_apply_h(mcpi_space sp, const void *d_C, void *d_out) { return apply_op(sp, sp ? sp->fwd : DevPairOp{}, d_C, d_out); }
+
+int mcpi_apply_h_profile(mcpi_space sp, const void *d_C, void *d_out, int reps, float *h_ms)
+{
+    CHECK_ARG(sp && d_C && d_out && h_ms && reps >= 1, "mcpi_apply_h_profile: bad arguments");
+    if (!sp->has_op) return fail(MCPI_ERR_STATE, "mcpi_set_integrals has not been called");
+    DeviceGuard g(sp->device);
+    int rc = ensure_E(sp);
+    if (rc) return rc;
+    cudaEvent_t ev[3];
+    for (auto &e : ev) CK(cudaEventCreate(&e));
+    float tot[2] = {0.f, 0.f};
+    cudaError_t e = cudaSuccess;
+    for (int r = 0; r < reps && e == cudaSuccess; ++r) {
+        e = cudaEventRecord(ev[0], sp->stream);
+        if (e == cudaSuccess)
+            e = mcpi::launch_apply_h(sp->sp, sp->tables(), sp->fwd.view(), sp->fwd.blocks(),
+                                     (const double2 *)d_C, sp->d_E, (double2 *)d_out, sp->stream, 1);
+        if (e == cudaSuccess) e = cudaEventRecord(ev[1], sp->stream);
+        if (e == cudaSuccess)
+            e = mcpi::launch_apply_h(sp->sp, sp->tables(), sp->fwd.view(), sp->fwd.blocks(),
+                                     (const double2 *)d_C, sp->d_E, (double2 *)d_out, sp->stream, 2);
+        if (e == cudaSuccess) e = cudaEventRecord(ev[2], sp->stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(ev[2]);
+        float a = 0.f, b = 0.f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&a, ev[0], ev[1]);
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&b, ev[1], ev[2]);
+        tot[0] += a;
+        tot[1] += b;
+    }
+    for (auto &x : ev) cudaEventDestroy(x);
+    if (e != cudaSuccess) return fail(MCPI_ERR_CUDA, "mcpi_apply_h_profile: %s", cudaGetErrorString(e));
+    h_ms[0] = tot[0] / reps;
+    h_ms[1] = tot[1] / reps;
+    return MCPI_OK;
+}
 
 int mcpi_apply_h_adjoint(mcpi_space sp, const void *d_C, void *d_out)
 {
@@ -600,16 +771,17 @@ int mcpi_lanczos(mcpi_space sp, void *d_lvec, int lm, double *h_diag, double *h_
     const int init[2] = {0, lm};
     double2 *V = (double2 *)d_lvec;
     const PairOp op = sp->fwd.view();
+    const mcpi::BlockOp bo = sp->fwd.blocks();
     const SpaceTables tb = sp->tables();
     e = cudaMemsetAsync(blk, 0, bytes, sp->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(s.done, init, sizeof init, cudaMemcpyHostToDevice, sp->stream);
-    if (e == cudaSuccess) e = mcpi::launch_apply_h(sp->sp, tb, op, V, sp->d_E, r, sp->stream);
+    if (e == cudaSuccess) e = mcpi::launch_apply_h(sp->sp, tb, op, bo, V, sp->d_E, r, sp->stream);
     if (e == cudaSuccess) e = mcpi::launch_lanczos_start(V, r, r, nc, s, sp->stream);
     for (int i = 0; i < lm - 1 && e == cudaSuccess; ++i) {
         double2 *vi = V + (size_t)i * nc, *vn = V + (size_t)(i + 1) * nc;
         e = mcpi::launch_lanczos_beta(i, lm, 1e-15, s, sp->stream);
         if (e == cudaSuccess) e = mcpi::launch_lanczos_scale(r, vn, nc, i, s, sp->stream);
-        if (e == cudaSuccess) e = mcpi::launch_apply_h(sp->sp, tb, op, vn, sp->d_E, r, sp->stream);
+        if (e == cudaSuccess) e = mcpi::launch_apply_h(sp->sp, tb, op, bo, vn, sp->d_E, r, sp->stream);
         if (e == cudaSuccess) e = mcpi::launch_lanczos_alpha(vi, vn, r, nc, i, s, sp->stream);
         if (e == cudaSuccess) e = mcpi::launch_lanczos_reorth(V, i + 2, r, nc, i, s, sp->stream);
     }
@@ -623,6 +795,8 @@ int mcpi_lanczos(mcpi_space sp, void *d_lvec, int lm, double *h_diag, double *h_
     cudaFree(blk);
     cudaFree(r);
     if (e != cudaSuccess) return fail(MCPI_ERR_CUDA, "mcpi_lanczos: %s", cudaGetErrorString(e));
+    rc = check_status(sp);
+    if (rc) return rc;
     if (h_diag) std::memcpy(h_diag, alpha.data(), sizeof(double2) * lm);
     if (h_offdiag) {
         for (int i = 0; i < lm; ++i) h_offdiag[i] = i < lm - 1 ? beta[i] : 0.0;

@@ -18,6 +18,27 @@ struct PairOp {
     const double2 *hdiag;   // M
     const double2 *hfull;   // M * M
     int nnz;
+    // momentum-block form (nullptr unless Ht only couples pairs of equal q + l):
+    // blocks K = 0 .. 2M-2 of the pairs (q, K-q), q = max(0,K-M+1) .. K/2, dense
+    // row-major values in that order
+    const double2 *hblk;
+    int nhblk;
+    int create_form;        // pair-creation kernel: 0 per-row tables in shared memory, 1 in registers
+    int *status;            // device status word (1: a bounded wait timed out)
+};
+
+// Block-sparse form of the same pair matrix: when Ht decomposes into blocks
+// (rows R_b x columns C_b, e.g. one block per total momentum for plane-wave
+// orbitals) with every |C_b| <= kBlockCols, kernel 1 keeps each block's
+// gathered column values in registers instead of staging all P of them.
+// One packed buffer: int header [nblocks, ncols_total, nrows_total, nvals],
+// then per block {col_begin, ncols, row_begin, nrows, val_begin}, then the
+// columns (q | l << 8), then the rows (pair index a), then (8-byte aligned)
+// the dense block values (row-major per block) as double2.
+constexpr int kBlockCols = 16;
+struct BlockOp {
+    const int *prog;        // packed buffer (nullptr: not block-sparse)
+    int bytes;              // size of the packed buffer
 };
 
 // Device tables of one space.
@@ -27,8 +48,11 @@ struct SpaceTables {
 };
 
 // H.psi : out = H psi. E is scratch of P * nc2 complex (unused when N < 2).
+// stages: bit 0 = kernel 1 (pair annihilation + pair matrix, writes E),
+//         bit 1 = kernel 2 (pair creation, reads E, writes out); 3 = both.
 cudaError_t launch_apply_h(const Space &sp, const SpaceTables &tb, const PairOp &op,
-                           const double2 *psi, double2 *E, double2 *out, cudaStream_t st);
+                           const BlockOp &bo, const double2 *psi, double2 *E, double2 *out,
+                           cudaStream_t st, int stages = 3);
 
 // Densities as Gram matrices over the (N-order)-particle space:
 // G[a][b] = sum_m conj(<m|A_a|phi>) <m|A_b|psi>, expanded to the reference

@@ -231,3 +231,23 @@ def test_lanczos_breakdown():
     assert it == 0
     E, psi, it2 = sp.ground(C0, 10)
     assert it2 == 0 and E == pytest.approx(diag[0].real)
+
+
+@pytest.mark.parametrize("N,M,g", [(8, 9, 2.5), (6, 11, 0.7), (5, 16, 1.0), (9, 7, 30.0)])
+def test_block_and_dense_pair_kernels_agree(orc, N, M, g):
+    # plane-wave integrals conserve momentum, so the pair matrix splits into
+    # one block per total momentum and the block-sparse kernel is used
+    Ho, Hint = mc.lieb_integrals(M, g)
+    C = mc.random_problem(N, M, 61)[0]
+    sp = _space(N, M)
+    sp.set_integrals(Ho, Hint)
+    fast = sp.apply_h(C).cpu().numpy()                 # momentum-block kernel
+    sp.set_momentum_kernel(False)
+    sp.set_integrals(Ho, Hint)
+    blocks = sp.apply_h(C).cpu().numpy()               # generic block-sparse kernel
+    sp.set_dense_pair_kernel(True)
+    sp.set_integrals(Ho, Hint)
+    dense = sp.apply_h(C).cpu().numpy()
+    ref = orc.apply_h(N, M, C, Ho, Hint, mode=2)
+    assert rel(fast, ref) <= TOL and rel(blocks, ref) <= TOL and rel(dense, ref) <= TOL
+    assert rel(sp.apply_h_adjoint(C).cpu().numpy(), ref) <= TOL    # Hermitian here
