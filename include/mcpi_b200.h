@@ -106,6 +106,21 @@ MCPI_API int mcpi_apply_h(mcpi_space sp, const void *d_C, void *d_out);
  * returns their mean durations in ms: h_ms[0] pair annihilation + pair-matrix
  * kernel, h_ms[1] pair creation kernel. For measurement, not for production. */
 MCPI_API int mcpi_apply_h_profile(mcpi_space sp, const void *d_C, void *d_out, int reps, float *h_ms);
+/* out = H C without allocating anything. No counterpart in the reference.
+ * For callers that cannot allocate device memory where they need H.psi (a
+ * host whose own pool allocator owns the GPU's memory, or a loop that cannot
+ * absorb cudaMalloc's synchronisation): it runs the H.psi kernels with all
+ * scratch taken from a 32 MiB array compiled into the library, which every GPU
+ * that loads the library holds until the process exits. Host integrals as in
+ * mcpi_set_integrals, device vectors d_C / d_out (nc complex), work enqueued on
+ * `stream` (a cudaStream_t, NULL = legacy default stream). Returns
+ * MCPI_ERR_RANGE, with nothing enqueued, when M > 10, N > 64 or the tables plus
+ * the P * NC(N-2,M) intermediate exceed the array (at M = 10: N <= 10).
+ * Calls share the array: calls that overlap on the GPU race. The first call
+ * on a device looks up the array's device address; make it before any stream
+ * capture begins. */
+MCPI_API int mcpi_apply_h_static(int N, int M, const double *h_Ho, const double *h_Hint, int variant,
+                                 const void *d_C, void *d_out, void *stream);
 /* out = H^dagger C (adjoint of the operator above; equal to H C when Ho is
  * Hermitian and Hint has the 8-fold symmetry). No reference counterpart. */
 MCPI_API int mcpi_apply_h_adjoint(mcpi_space sp, const void *d_C, void *d_out);
