@@ -73,6 +73,13 @@ MCPI_API int mcpi_space_sync(mcpi_space sp);
 #define MCPI_OPT_CREATE_FORM 3
 MCPI_API int mcpi_space_set_option(mcpi_space sp, int option, int value);
 MCPI_API int mcpi_space_dims(mcpi_space sp, int *N, int *M, int64_t *nc);
+/* Device memory on the space's device, and a synchronous copy in any direction
+ * (host or device pointers, on the space's stream), for hosts without CUDA
+ * headers. Replace the reference's malloc'd arrays that must live on the GPU
+ * (configurationsMap.h:46-116 rarrDef/carrDef/iarrDef). */
+MCPI_API int mcpi_alloc(mcpi_space sp, size_t bytes, void **d_ptr);
+MCPI_API int mcpi_free(mcpi_space sp, void *d_ptr);
+MCPI_API int mcpi_memcpy(mcpi_space sp, void *dst, const void *src, size_t bytes);
 
 /* ---- tables in the reference layouts, built on the device ---------------- */
 /* NCmat[n + (N+1)*m] = NC(n,m), host output (configurationsMap.h:206-234). */

@@ -360,6 +360,8 @@ int apply_op(mcpi_space_s *sp, const DevPairOp &op, const void *d_C, void *d_out
 
 extern "C" {
 
+static int check_status(mcpi_space_s *sp);
+
 const char *mcpi_status_string(int status)
 {
     switch (status) {
@@ -502,6 +504,32 @@ int mcpi_space_sync(mcpi_space sp)
 {
     CHECK_ARG(sp, "null space");
     DeviceGuard g(sp->device);
+    CK(cudaStreamSynchronize(sp->stream));
+    return check_status(sp);
+}
+
+int mcpi_alloc(mcpi_space sp, size_t bytes, void **d_ptr)
+{
+    CHECK_ARG(sp && d_ptr, "null argument");
+    DeviceGuard g(sp->device);
+    *d_ptr = nullptr;
+    CK(cudaMalloc(d_ptr, bytes ? bytes : 1));
+    return MCPI_OK;
+}
+
+int mcpi_free(mcpi_space sp, void *d_ptr)
+{
+    CHECK_ARG(sp, "null space");
+    DeviceGuard g(sp->device);
+    CK(cudaFree(d_ptr));
+    return MCPI_OK;
+}
+
+int mcpi_memcpy(mcpi_space sp, void *dst, const void *src, size_t bytes)
+{
+    CHECK_ARG(sp && (bytes == 0 || (dst && src)), "null argument");
+    DeviceGuard g(sp->device);
+    CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, sp->stream));
     CK(cudaStreamSynchronize(sp->stream));
     return check_status(sp);
 }

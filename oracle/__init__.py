@@ -40,6 +40,8 @@ def build(ref: bool = True) -> None:
     targets = ["liborc.so"]
     if ref and os.path.exists(os.path.join(REFERENCE_SRC, "configurationsMap.h")):
         targets.append("ref")
+        if os.path.exists(os.path.join(HERE, "..", "mcpi_b200", "libmcpi_dropin.so")):
+            targets.append("dropin")
     subprocess.run(["make", "-s", "-C", HERE, f"REF={REFERENCE_SRC}", *targets], check=True)
 
 

@@ -16,7 +16,8 @@ HEADERS = [os.path.join(ROOT, "include", h) for h in os.listdir(os.path.join(ROO
 
 def _declared(path):
     text = open(path).read()
-    return set(re.findall(r"^MCPI_API\s+[\w\s\*]*?\b(\w+)\s*\(", text, flags=re.M))
+    return set(re.findall(r"^(?:MCPI_API|MCPI_DROPIN_API)\s+[\w\s\*]*?\b(\w+)\s*\(", text,
+                          flags=re.M))
 
 
 def _lib_for(header):
