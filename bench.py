@@ -53,6 +53,7 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-lanczos", action="store_true")
+    p.add_argument("--no-batch", action="store_true")
     return p.parse_args()
 
 
@@ -148,6 +149,58 @@ def hpsi_bytes(nc, nc2, P):
 # ---------------------------------------------------------------------------
 # CPU baseline: oracle restatement of applyHconf_X on a row sample
 # ---------------------------------------------------------------------------
+
+def batch_members(count=64, seed=2024):
+    """The batched sweep: g log-uniform in [0.01, 100], N uniform in 6..14,
+    M uniform in {7, 9, 11}, from one fixed seed."""
+    rng = np.random.default_rng(seed)
+    N = rng.integers(6, 15, count)
+    M = rng.choice([7, 9, 11], count)
+    g = 10.0 ** rng.uniform(-2.0, 2.0, count)
+    return [(int(n), int(m), float(x)) for n, m, x in zip(N, M, g)]
+
+
+def run_batch(mc, torch, device, iters=120):
+    """64 Lieb-Liniger solves: one graph-captured batch against one solve at a time."""
+    members = batch_members()
+    starts = []
+    b = mc.Batch([(n, m) for n, m, _ in members], iters, device=device)
+    for k, (n, m, g) in enumerate(members):
+        b.set_integrals(k, *mc.lieb_integrals(m, g, L_RING))
+        rng = np.random.default_rng(300 + k)
+        C = rng.standard_normal(b.nc[k]) + 1j * rng.standard_normal(b.nc[k])
+        C /= np.linalg.norm(C)
+        starts.append(C)
+        b.set_start(k, C)
+    b.run()                                   # capture + instantiate + one run
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    E, it = b.run()
+    t_batch = time.perf_counter() - t0
+    arena = b.arena_bytes()
+    b.close()
+    spaces = []
+    for k, (n, m, g) in enumerate(members):
+        sp = mc.FockSpace(n, m, device=device)
+        sp.set_integrals(*mc.lieb_integrals(m, g, L_RING))
+        spaces.append((sp, torch.from_numpy(starts[k]).to(sp.torch_device)))
+    sp0, c0 = spaces[0]
+    sp0.ground(c0, iters)                      # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    Es = [sp.ground(c, iters)[0] for sp, c in spaces]
+    torch.cuda.synchronize()
+    t_seq = time.perf_counter() - t0
+    for sp, _ in spaces:
+        sp.close()
+    dE = float(np.max(np.abs(np.array(Es) - E) / np.maximum(1.0, np.abs(np.array(Es)))))
+    ncs = [mc.nc_of(n, m) for n, m, _ in members]
+    return {"members": len(members), "iterations": iters, "solves_per_s": len(members) / t_batch,
+            "seconds": t_batch, "sequential_solves_per_s": len(members) / t_seq,
+            "sequential_seconds": t_seq, "speedup_vs_sequential": t_seq / t_batch,
+            "max_rel_dE0_vs_sequential": dE, "steps_done_min": int(it.min()),
+            "nc_min": min(ncs), "nc_max": max(ncs), "arena_gb": arena / 1e9}
+
 
 def cpu_setup(N, M, g):
     import oracle
@@ -349,6 +402,10 @@ def run_mcpi(args):
         lanczos = {"iterations": it, "E0": E0, "E0_per_N": E0 / N, "seconds": dt,
                    "solves_per_s": world / dt, "occupations": [round(float(o), 6) for o in occ]}
 
+    batched = None
+    if not args.no_batch:
+        batched = run_batch(mc, torch, local)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args.cpu_seconds)
@@ -358,7 +415,7 @@ def run_mcpi(args):
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
                 "config": config(), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-                "gpu_launches": 2 * args.steps, "clocks": clk, "lanczos": lanczos}
+                "gpu_launches": 2 * args.steps, "clocks": clk, "lanczos": lanczos, "batched": batched}
         print(json.dumps(line), flush=True)
     sp.close()
     if world > 1:

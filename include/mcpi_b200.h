@@ -160,6 +160,30 @@ MCPI_API int mcpi_ground(mcpi_space sp, void *d_C, int niter, double *E0, int *i
  * used at groundStateLieb.c:435. Host arrays. */
 MCPI_API int mcpi_tridiag_eig(int n, double *d, double *e, double *z);
 
+/* ---- batched ground states (no reference counterpart) ----------------------- */
+/* Many Lanczos ground-state solves of different (N, M) in one device arena,
+ * advanced together and replayed as one CUDA graph: each Lanczos stage is one
+ * launch over all members, every member keeps the reference recurrence
+ * (groundStateLieb.c:217-344: full CGS reorthogonalisation, breakdown test),
+ * and the lowest eigenvalue of each tridiagonal is found on the device by
+ * Sturm bisection. lm = Lanczos steps per member (2 .. 2048). Members need
+ * N >= 2, 2 <= M <= 16 and integrals that conserve the total orbital index
+ * (plane-wave integrals of a translation-invariant interaction, e.g.
+ * mcpi_lieb_integrals). The batch changes the calling thread's current device. */
+typedef struct mcpi_batch_s *mcpi_batch;
+MCPI_API int mcpi_batch_create(int count, const int *N, const int *M, int lm, int device, mcpi_batch *out);
+MCPI_API int mcpi_batch_member_size(mcpi_batch b, int member, int64_t *nc);
+MCPI_API int mcpi_batch_set_integrals(mcpi_batch b, int member, const double *h_Ho, const double *h_Hint,
+                                      int variant);
+/* Start vector of a member (host or device pointer, nc complex); kept for
+ * every later mcpi_batch_run. */
+MCPI_API int mcpi_batch_set_start(mcpi_batch b, int member, const void *C);
+/* Runs all members (the first call captures and instantiates the graph) and
+ * returns each member's lowest eigenvalue and Lanczos step count. */
+MCPI_API int mcpi_batch_run(mcpi_batch b, double *h_E0, int *h_iters);
+MCPI_API int mcpi_batch_arena_bytes(mcpi_batch b, size_t *bytes);
+MCPI_API int mcpi_batch_destroy(mcpi_batch b);
+
 /* ---- model inputs ------------------------------------------------------------ */
 /* Lieb-Liniger plane-wave integrals on a ring of length L
  * (groundStateLieb.c:129-213, setupHo / setupHint), host outputs. */

@@ -85,6 +85,13 @@ def lib():
         "mcpi_ground": (i, [_vp, _vp, i, pd, pi]),
         "mcpi_tridiag_eig": (i, [i, _vp, _vp, _vp]),
         "mcpi_lieb_integrals": (i, [i, d, d, _vp, _vp]),
+        "mcpi_batch_create": (i, [i, _vp, _vp, i, i, ct.POINTER(_vp)]),
+        "mcpi_batch_member_size": (i, [_vp, i, p64]),
+        "mcpi_batch_set_integrals": (i, [_vp, i, _vp, _vp, i]),
+        "mcpi_batch_set_start": (i, [_vp, i, _vp]),
+        "mcpi_batch_run": (i, [_vp, _vp, _vp]),
+        "mcpi_batch_arena_bytes": (i, [_vp, ct.POINTER(ct.c_size_t)]),
+        "mcpi_batch_destroy": (i, [_vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -346,6 +353,61 @@ class FockSpace:
         self._stream()
         _check(lib().mcpi_ground(self._h, _vp(C.data_ptr()), niter, ct.byref(E), ct.byref(it)))
         return E.value, C, it.value
+
+
+class Batch:
+    """Many Lanczos ground-state solves advanced together and replayed as one
+    CUDA graph (mcpi_batch_* in mcpi_b200.h). members: list of (N, M)."""
+
+    def __init__(self, members, lm: int, device: int = 0):
+        self.members = list(members)
+        n = len(self.members)
+        Ns = np.array([m[0] for m in self.members], np.int32)
+        Ms = np.array([m[1] for m in self.members], np.int32)
+        h = _vp()
+        _check(lib().mcpi_batch_create(n, _np_ptr(Ns), _np_ptr(Ms), lm, device, ct.byref(h)))
+        self._h = h
+        self.lm = lm
+        self.nc = []
+        for k in range(n):
+            v = ct.c_int64(0)
+            _check(lib().mcpi_batch_member_size(self._h, k, ct.byref(v)))
+            self.nc.append(v.value)
+
+    def set_integrals(self, k, Ho, Hint, variant=VARIANT_MAPS):
+        N, M = self.members[k]
+        Ho = np.ascontiguousarray(np.asarray(Ho, np.complex128).reshape(M, M))
+        Hint = np.ascontiguousarray(np.asarray(Hint, np.complex128).reshape(-1))
+        _check(lib().mcpi_batch_set_integrals(self._h, k, _np_ptr(Ho), _np_ptr(Hint), int(variant)))
+
+    def set_start(self, k, C):
+        C = np.ascontiguousarray(C, np.complex128)
+        if C.size != self.nc[k]:
+            raise MCPIError(1, "start vector has the wrong length")
+        _check(lib().mcpi_batch_set_start(self._h, k, _np_ptr(C)))
+
+    def run(self):
+        """Returns (E0 per member, Lanczos steps per member)."""
+        E = np.zeros(len(self.members))
+        it = np.zeros(len(self.members), np.int32)
+        _check(lib().mcpi_batch_run(self._h, _np_ptr(E), _np_ptr(it)))
+        return E, it
+
+    def arena_bytes(self) -> int:
+        v = ct.c_size_t(0)
+        _check(lib().mcpi_batch_arena_bytes(self._h, ct.byref(v)))
+        return v.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().mcpi_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 # ---------------------------------------------------------------------------

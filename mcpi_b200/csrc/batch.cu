@@ -1,0 +1,596 @@
+// Batched Lanczos: many ground-state solves of different (N, M) advanced
+// together in one device arena and replayed as one CUDA graph.
+//
+// Reference: groundStateLieb.c runs one solve at a time (lanczos :217-344,
+// ground :348-471) with host dots and a host tridiagonal solve. Here every
+// member keeps the reference's recurrence (full classical Gram-Schmidt
+// reorthogonalisation, breakdown at beta_i / max beta < 1e-15) but each
+// stage is one launch over all members:
+//   * H.psi: one annihilation + one creation launch per orbital count M
+//     (hpsi.cu, k_batch_*), blocks assigned from (member, block) work tables;
+//   * vector stages: blocks assigned from (member, 2048-row tile) work tables,
+//     per-member partial sums reduced in a fixed order by one block per member;
+//   * a member whose Lanczos broke down sets its flag and every later block of
+//     that member returns at entry (per-member masking);
+//   * the lowest eigenvalue of each member's tridiagonal is found on the
+//     device by Sturm-sequence bisection (Barth, Martin & Wilkinson 1967), so
+//     the whole solve -- start vectors, 120 steps, eigenvalues -- is captured
+//     once and replayed with a single cudaGraphLaunch.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "kernels.h"
+#include "space.h"
+
+namespace mcpi {
+
+struct BatchLz {
+    int64_t nc;
+    double2 *V;        // lm * nc Krylov basis
+    double2 *r;        // nc residual (H.psi output)
+    double2 *alpha;    // lm
+    double *beta;      // lm
+    double *maxbeta;   // 1
+    int *done;         // 1
+    int *iters;        // 1
+    double2 *coef;     // lm
+    double2 *part;     // (lm + 1) * ntiles partial sums
+    int ntiles;        // ceil(nc / kTileRows)
+};
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kTileRows = 2048;
+
+__device__ __forceinline__ double2 warp_sum2(double2 v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        v.x += __shfl_down_sync(0xffffffffu, v.x, o);
+        v.y += __shfl_down_sync(0xffffffffu, v.y, o);
+    }
+    return v;
+}
+
+// fixed-order block sum, result in thread 0
+__device__ __forceinline__ double2 block_sum2(double2 v)
+{
+    __shared__ double2 red[kThreads / 32];
+    v = warp_sum2(v);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x / 32] = v;
+    __syncthreads();
+    double2 r = make_double2(0.0, 0.0);
+    if (threadIdx.x == 0)
+        for (int k = 0; k < kThreads / 32; ++k) {
+            r.x += red[k].x;
+            r.y += red[k].y;
+        }
+    return r;
+}
+
+__device__ __forceinline__ double2 cmulc(double2 a, double2 b)  // conj(a) b
+{
+    return make_double2(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x);
+}
+
+__global__ void kb_reset(BatchLz *L, int nmem, int lm)
+{
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= nmem) return;
+    *L[m].maxbeta = 0.0;
+    *L[m].done = 0;
+    *L[m].iters = lm;
+}
+
+// partial of <V_a, r> over one tile; with beta_i set, r -= beta_i V_prev first
+__global__ void kb_axpy_dot(BatchLz *L, const int2 *__restrict__ work, int i)
+{
+    const int2 w = work[blockIdx.x];
+    BatchLz &b = L[w.x];
+    if (*b.done) return;
+    const int64_t r0 = (int64_t)w.y * kTileRows;
+    const int64_t r1 = min(b.nc, r0 + kTileRows);
+    const double2 *va = b.V + (size_t)(i + 1) * b.nc;
+    const double2 *vp = i >= 0 ? b.V + (size_t)i * b.nc : nullptr;
+    const double bi = i >= 0 ? b.beta[i] : 0.0;
+    double2 acc = make_double2(0.0, 0.0);
+    for (int64_t x = r0 + threadIdx.x; x < r1; x += kThreads) {
+        double2 y = b.r[x];
+        if (vp) {
+            const double2 p = vp[x];
+            y.x -= bi * p.x;
+            y.y -= bi * p.y;
+            b.r[x] = y;
+        }
+        const double2 d = cmulc(va[x], y);
+        acc.x += d.x;
+        acc.y += d.y;
+    }
+    acc = block_sum2(acc);
+    if (threadIdx.x == 0) b.part[w.y] = acc;
+}
+
+// alpha[k] = sum of the member's tile partials (one block per member)
+__global__ void kb_sum_alpha(BatchLz *L, int k)
+{
+    BatchLz &b = L[blockIdx.x];
+    if (*b.done) return;
+    double2 acc = make_double2(0.0, 0.0);
+    for (int t = threadIdx.x; t < b.ntiles; t += kThreads) {
+        acc.x += b.part[t].x;
+        acc.y += b.part[t].y;
+    }
+    acc = block_sum2(acc);
+    if (threadIdx.x == 0) b.alpha[k] = acc;
+}
+
+// part[j * ntiles + tile] = <V_j, r - alpha_cur V_cur> over the tile, j < nvec
+__global__ void __launch_bounds__(kThreads) kb_multidot(BatchLz *L, const int2 *__restrict__ work,
+                                                        int cur, int nvec)
+{
+    __shared__ double2 xs[kTileRows];
+    const int2 w = work[blockIdx.x];
+    BatchLz &b = L[w.x];
+    if (*b.done) return;
+    const int64_t r0 = (int64_t)w.y * kTileRows;
+    const int rows = (int)min((int64_t)kTileRows, b.nc - r0);
+    const double2 a = b.alpha[cur];
+    const double2 *vc = b.V + (size_t)cur * b.nc + r0;
+    for (int t = threadIdx.x; t < rows; t += kThreads) {
+        const double2 y = b.r[r0 + t], v = vc[t];
+        xs[t] = make_double2(y.x - (a.x * v.x - a.y * v.y), y.y - (a.x * v.y + a.y * v.x));
+    }
+    __syncthreads();
+    const int wid = threadIdx.x / 32, lane = threadIdx.x % 32;
+    for (int j = wid; j < nvec; j += kThreads / 32) {
+        const double2 *vj = b.V + (size_t)j * b.nc + r0;
+        double2 acc = make_double2(0.0, 0.0);
+#pragma unroll 4
+        for (int t = lane; t < rows; t += 32) {
+            const double2 p = cmulc(vj[t], xs[t]);
+            acc.x += p.x;
+            acc.y += p.y;
+        }
+        acc = warp_sum2(acc);
+        if (lane == 0) b.part[(size_t)j * b.ntiles + w.y] = acc;
+    }
+}
+
+// coef[j] = sum over tiles (one block per member, one warp per j)
+__global__ void kb_coef(BatchLz *L, int nvec)
+{
+    BatchLz &b = L[blockIdx.x];
+    if (*b.done) return;
+    const int wid = threadIdx.x / 32, lane = threadIdx.x % 32;
+    for (int j = wid; j < nvec; j += kThreads / 32) {
+        double2 acc = make_double2(0.0, 0.0);
+        for (int t = lane; t < b.ntiles; t += 32) {
+            acc.x += b.part[(size_t)j * b.ntiles + t].x;
+            acc.y += b.part[(size_t)j * b.ntiles + t].y;
+        }
+        acc = warp_sum2(acc);
+        if (lane == 0) b.coef[j] = acc;
+    }
+}
+
+// r = (r - alpha_cur V_cur) - sum_{j<nvec} coef_j V_j ; part[tile] = |r|^2 over the tile
+__global__ void __launch_bounds__(kThreads) kb_update(BatchLz *L, const int2 *__restrict__ work,
+                                                      int cur, int nvec)
+{
+    extern __shared__ double2 cs[];
+    const int2 w = work[blockIdx.x];
+    BatchLz &b = L[w.x];
+    if (*b.done) return;
+    for (int j = threadIdx.x; j < nvec; j += kThreads) cs[j] = b.coef[j];
+    __syncthreads();
+    const int64_t r0 = (int64_t)w.y * kTileRows;
+    const int64_t r1 = min(b.nc, r0 + kTileRows);
+    const double2 a = b.alpha[cur];
+    const double2 *vc = b.V + (size_t)cur * b.nc;
+    double acc = 0.0;
+    for (int64_t x = r0 + threadIdx.x; x < r1; x += kThreads) {
+        const double2 y = b.r[x], v = vc[x];
+        double2 u = make_double2(y.x - (a.x * v.x - a.y * v.y), y.y - (a.x * v.y + a.y * v.x));
+        for (int j = 0; j < nvec; ++j) {
+            const double2 p = b.V[(size_t)j * b.nc + x], c = cs[j];
+            u.x -= p.x * c.x - p.y * c.y;
+            u.y -= p.x * c.y + p.y * c.x;
+        }
+        b.r[x] = u;
+        acc += u.x * u.x + u.y * u.y;
+    }
+    const double2 s = block_sum2(make_double2(acc, 0.0));
+    if (threadIdx.x == 0) b.part[w.y] = s;
+}
+
+// beta_i and the breakdown test of groundStateLieb.c:287-292 (one block per member)
+__global__ void kb_beta(BatchLz *L, int i, double tol)
+{
+    BatchLz &b = L[blockIdx.x];
+    if (*b.done) return;
+    double2 acc = make_double2(0.0, 0.0);
+    for (int t = threadIdx.x; t < b.ntiles; t += kThreads) acc.x += b.part[t].x;
+    acc = block_sum2(acc);
+    if (threadIdx.x == 0) {
+        const double bi = sqrt(acc.x);
+        b.beta[i] = bi;
+        if (*b.maxbeta < bi) *b.maxbeta = bi;
+        if (!(bi / *b.maxbeta >= tol)) {
+            *b.done = 1;
+            *b.iters = i;
+        }
+    }
+}
+
+__global__ void kb_scale(BatchLz *L, const int2 *__restrict__ work, int i)
+{
+    const int2 w = work[blockIdx.x];
+    BatchLz &b = L[w.x];
+    if (*b.done) return;
+    const int64_t r0 = (int64_t)w.y * kTileRows;
+    const int64_t r1 = min(b.nc, r0 + kTileRows);
+    const double bi = b.beta[i];
+    double2 *vn = b.V + (size_t)(i + 1) * b.nc;
+    for (int64_t x = r0 + threadIdx.x; x < r1; x += kThreads) {
+        const double2 y = b.r[x];
+        vn[x] = make_double2(y.x / bi, y.y / bi);
+    }
+}
+
+// Number of eigenvalues of the tridiagonal (d, e) below x (Sturm sequence).
+__device__ int sturm_count(const double2 *alpha, const double *beta, int n, double x)
+{
+    int c = 0;
+    double q = 1.0;
+    for (int k = 0; k < n; ++k) {
+        const double e2 = k > 0 ? beta[k - 1] * beta[k - 1] : 0.0;
+        q = alpha[k].x - x - (k > 0 ? e2 / q : 0.0);
+        if (q == 0.0) q = -1e-300;   // step off an exact pole
+        c += q < 0.0;
+    }
+    return c;
+}
+
+// Lowest eigenvalue of each member's tridiagonal by bisection on the Sturm
+// count, from Gershgorin bounds to the resolution of double precision.
+__global__ void kb_eig(BatchLz *L, int nmem, double *E0, int *iters)
+{
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= nmem) return;
+    BatchLz &b = L[m];
+    const int it = *b.iters;
+    const int n = it > 0 ? it : 1;
+    double lo = 1e300, hi = -1e300;
+    for (int k = 0; k < n; ++k) {
+        const double rad = (k > 0 ? fabs(b.beta[k - 1]) : 0.0) + (k + 1 < n ? fabs(b.beta[k]) : 0.0);
+        lo = fmin(lo, b.alpha[k].x - rad);
+        hi = fmax(hi, b.alpha[k].x + rad);
+    }
+    for (int s = 0; s < 200 && hi - lo > 2.2e-16 * fmax(fabs(lo), fabs(hi)) + 1e-300; ++s) {
+        const double mid = 0.5 * (lo + hi);
+        if (mid <= lo || mid >= hi) break;
+        if (sturm_count(b.alpha, b.beta, n, mid) >= 1) hi = mid;
+        else lo = mid;
+    }
+    E0[m] = 0.5 * (lo + hi);
+    iters[m] = it;
+}
+
+size_t up256(size_t x) { return (x + 255) & ~size_t(255); }
+
+}  // namespace
+}  // namespace mcpi
+
+using mcpi::BatchLz;
+using mcpi::BatchMember;
+
+struct mcpi_batch_s {
+    int count = 0, lm = 0, device = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<mcpi_space> spaces;
+    std::vector<BatchLz> lz;
+    std::vector<BatchMember> mem;
+    std::vector<double2 *> start;
+    char *arena = nullptr;
+    char *meta = nullptr;   // device copies of lz, mem, work tables, results
+    BatchLz *d_lz = nullptr;
+    BatchMember *d_mem = nullptr;
+    int2 *d_vwork = nullptr;
+    int nvwork = 0;
+    struct Group {
+        int M;
+        int2 *w1, *w2;
+        int n1, n2;
+        size_t sm1, sm2;
+    };
+    std::vector<Group> groups;
+    double *d_E0 = nullptr;
+    int *d_iters = nullptr;
+    std::vector<char> ready;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    size_t arena_bytes = 0;
+};
+
+namespace {
+
+int bfail(int code, const std::string &msg) { return mcpi::set_error(code, msg.c_str()); }
+
+}  // namespace
+
+extern "C" {
+
+int mcpi_batch_create(int count, const int *N, const int *M, int lm, int device, mcpi_batch *out)
+{
+    if (!out || !N || !M || count < 1 || lm < 2 || lm > 2048)
+        return bfail(MCPI_ERR_ARG, "mcpi_batch_create: bad arguments");
+    *out = nullptr;
+    if (cudaSetDevice(device) != cudaSuccess) return bfail(MCPI_ERR_CUDA, "mcpi_batch_create: bad device");
+    auto *b = new mcpi_batch_s;
+    b->count = count;
+    b->lm = lm;
+    b->device = device;
+    b->spaces.assign(count, nullptr);
+    b->ready.assign(count, 0);
+    auto cleanup = [&](int rc, const std::string &msg) {
+        mcpi_batch_destroy(b);
+        return bfail(rc, msg);
+    };
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return cleanup(MCPI_ERR_CUDA, "stream creation failed");
+    // sizes
+    std::vector<size_t> off_V(count), off_r(count), off_E(count), off_S(count), off_st(count);
+    size_t tot = 0;
+    b->lz.resize(count);
+    b->mem.resize(count);
+    for (int m = 0; m < count; ++m) {
+        if (N[m] < 2 || M[m] < 2 || M[m] > mcpi::kMaxM)
+            return cleanup(MCPI_ERR_RANGE, "batched members need N >= 2 and 2 <= M <= 16");
+        int rc = mcpi_space_create(N[m], M[m], device, &b->spaces[m]);
+        if (rc) return cleanup(rc, std::string("member space: ") + mcpi_last_error());
+        const mcpi_space_s *s = b->spaces[m];
+        const int64_t nc = s->nc;
+        const int ntiles = (int)((nc + mcpi::kTileRows - 1) / mcpi::kTileRows);
+        b->lz[m].nc = nc;
+        b->lz[m].ntiles = ntiles;
+        off_V[m] = tot;
+        tot += mcpi::up256(sizeof(double2) * (size_t)lm * nc);
+        off_r[m] = tot;
+        tot += mcpi::up256(sizeof(double2) * nc);
+        off_E[m] = tot;
+        tot += mcpi::up256(sizeof(double2) * (size_t)s->P * s->nc2);
+        off_S[m] = tot;
+        tot += mcpi::up256(sizeof(double2) * nc);
+        off_st[m] = tot;
+        tot += mcpi::up256(sizeof(double2) * (2 * (size_t)lm + (size_t)(lm + 1) * ntiles) +
+                           sizeof(double) * (lm + 1) + 2 * sizeof(int));
+    }
+    if (cudaMalloc(&b->arena, tot) != cudaSuccess)
+        return cleanup(MCPI_ERR_NOMEM, "arena allocation failed (" + std::to_string(tot) + " bytes)");
+    b->arena_bytes = tot;
+    b->start.resize(count);
+    for (int m = 0; m < count; ++m) {
+        BatchLz &z = b->lz[m];
+        const mcpi_space_s *s = b->spaces[m];
+        z.V = reinterpret_cast<double2 *>(b->arena + off_V[m]);
+        z.r = reinterpret_cast<double2 *>(b->arena + off_r[m]);
+        b->start[m] = reinterpret_cast<double2 *>(b->arena + off_S[m]);
+        char *st = b->arena + off_st[m];
+        z.alpha = reinterpret_cast<double2 *>(st);
+        z.coef = z.alpha + lm;
+        z.part = z.coef + lm;
+        z.beta = reinterpret_cast<double *>(z.part + (size_t)(lm + 1) * z.ntiles);
+        z.maxbeta = z.beta + lm;
+        z.done = reinterpret_cast<int *>(z.maxbeta + 1);
+        z.iters = z.done + 1;
+        BatchMember &bm = b->mem[m];
+        bm.sp = s->sp;
+        bm.W = s->d_W;
+        bm.sq = s->d_sq;
+        bm.hblk = nullptr;
+        bm.nh = 0;
+        bm.hdiag = nullptr;
+        bm.lvec = z.V;
+        bm.E = reinterpret_cast<double2 *>(b->arena + off_E[m]);
+        bm.r = z.r;
+        bm.done = z.done;
+    }
+    // work tables: vector tiles of every member, H.psi blocks grouped by M
+    std::vector<int2> vwork;
+    for (int m = 0; m < count; ++m)
+        for (int t = 0; t < b->lz[m].ntiles; ++t) vwork.push_back(make_int2(m, t));
+    std::vector<int> Ms(M, M + count);
+    std::sort(Ms.begin(), Ms.end());
+    Ms.erase(std::unique(Ms.begin(), Ms.end()), Ms.end());
+    std::vector<std::vector<int2>> w1(Ms.size()), w2(Ms.size());
+    const int rpb = mcpi::batch_rows_per_block();
+    for (size_t g = 0; g < Ms.size(); ++g)
+        for (int m = 0; m < count; ++m) {
+            if (M[m] != Ms[g]) continue;
+            const mcpi_space_s *s = b->spaces[m];
+            for (int64_t k = 0; k < (s->nc2 + rpb - 1) / rpb; ++k) w1[g].push_back(make_int2(m, (int)k));
+            for (int64_t k = 0; k < (s->nc + rpb - 1) / rpb; ++k) w2[g].push_back(make_int2(m, (int)k));
+        }
+    size_t mbytes = mcpi::up256(sizeof(BatchLz) * count) + mcpi::up256(sizeof(BatchMember) * count) +
+                    mcpi::up256(sizeof(int2) * vwork.size()) + mcpi::up256(sizeof(double) * count) +
+                    mcpi::up256(sizeof(int) * count);
+    for (size_t g = 0; g < Ms.size(); ++g)
+        mbytes += mcpi::up256(sizeof(int2) * w1[g].size()) + mcpi::up256(sizeof(int2) * w2[g].size());
+    if (cudaMalloc(&b->meta, mbytes) != cudaSuccess) return cleanup(MCPI_ERR_NOMEM, "metadata allocation failed");
+    char *p = b->meta;
+    auto take = [&](size_t bytes) {
+        char *q = p;
+        p += mcpi::up256(bytes);
+        return q;
+    };
+    b->d_lz = reinterpret_cast<BatchLz *>(take(sizeof(BatchLz) * count));
+    b->d_mem = reinterpret_cast<BatchMember *>(take(sizeof(BatchMember) * count));
+    b->d_vwork = reinterpret_cast<int2 *>(take(sizeof(int2) * vwork.size()));
+    b->nvwork = (int)vwork.size();
+    b->d_E0 = reinterpret_cast<double *>(take(sizeof(double) * count));
+    b->d_iters = reinterpret_cast<int *>(take(sizeof(int) * count));
+    cudaError_t e = cudaMemcpy(b->d_lz, b->lz.data(), sizeof(BatchLz) * count, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(b->d_vwork, vwork.data(), sizeof(int2) * vwork.size(), cudaMemcpyHostToDevice);
+    for (size_t g = 0; g < Ms.size() && e == cudaSuccess; ++g) {
+        mcpi_batch_s::Group G{};
+        G.M = Ms[g];
+        G.w1 = reinterpret_cast<int2 *>(take(sizeof(int2) * w1[g].size()));
+        G.w2 = reinterpret_cast<int2 *>(take(sizeof(int2) * w2[g].size()));
+        G.n1 = (int)w1[g].size();
+        G.n2 = (int)w2[g].size();
+        int maxN = 0;
+        for (int m = 0; m < count; ++m)
+            if (M[m] == Ms[g]) maxN = std::max(maxN, N[m]);
+        const int P = Ms[g] * (Ms[g] + 1) / 2;
+        int nh = 0;   // momentum-block values: sum over K of (block size)^2
+        for (int K = 0; K <= 2 * Ms[g] - 2; ++K) {
+            const int qlo = std::max(0, K - (Ms[g] - 1)), n = K / 2 - qlo + 1;
+            nh += n * n;
+        }
+        (void)P;
+        G.sm1 = mcpi::batch_smem(Ms[g], maxN, nh, 1);
+        G.sm2 = mcpi::batch_smem(Ms[g], maxN, nh, 2);
+        e = mcpi::batch_prepare(Ms[g], G.sm1, G.sm2);
+        if (e != cudaSuccess) break;
+        e = cudaMemcpy(G.w1, w1[g].data(), sizeof(int2) * w1[g].size(), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(G.w2, w2[g].data(), sizeof(int2) * w2[g].size(), cudaMemcpyHostToDevice);
+        b->groups.push_back(G);
+    }
+    if (e != cudaSuccess) return cleanup(MCPI_ERR_CUDA, std::string("upload: ") + cudaGetErrorString(e));
+    *out = b;
+    return MCPI_OK;
+}
+
+int mcpi_batch_member_size(mcpi_batch b, int member, int64_t *nc)
+{
+    if (!b || member < 0 || member >= b->count || !nc) return bfail(MCPI_ERR_ARG, "bad arguments");
+    *nc = b->lz[member].nc;
+    return MCPI_OK;
+}
+
+int mcpi_batch_set_integrals(mcpi_batch b, int member, const double *h_Ho, const double *h_Hint, int variant)
+{
+    if (!b || member < 0 || member >= b->count) return bfail(MCPI_ERR_ARG, "bad member");
+    int rc = mcpi_set_integrals(b->spaces[member], h_Ho, h_Hint, variant);
+    if (rc) return bfail(rc, mcpi_last_error());
+    const mcpi_space_s *s = b->spaces[member];
+    if (!s->fwd.hblk)
+        return bfail(MCPI_ERR_ARG, "batched solves need integrals that conserve the total orbital index "
+                                   "(momentum-conserving plane-wave integrals)");
+    BatchMember &bm = b->mem[member];
+    bm.hblk = s->fwd.hblk;
+    bm.nh = s->fwd.nhblk;
+    bm.hdiag = s->fwd.hdiag;
+    b->ready[member] |= 1;
+    if (cudaMemcpy(b->d_mem + member, &bm, sizeof(BatchMember), cudaMemcpyHostToDevice) != cudaSuccess)
+        return bfail(MCPI_ERR_CUDA, "member upload failed");
+    return MCPI_OK;
+}
+
+int mcpi_batch_set_start(mcpi_batch b, int member, const void *C)
+{
+    if (!b || member < 0 || member >= b->count || !C) return bfail(MCPI_ERR_ARG, "bad arguments");
+    if (cudaSetDevice(b->device) != cudaSuccess ||
+        cudaMemcpy(b->start[member], C, sizeof(double2) * b->lz[member].nc, cudaMemcpyDefault) != cudaSuccess)
+        return bfail(MCPI_ERR_CUDA, "start vector copy failed");
+    b->ready[member] |= 2;
+    return MCPI_OK;
+}
+
+static cudaError_t enqueue_solve(mcpi_batch b)
+{
+    cudaStream_t st = b->stream;
+    const int lm = b->lm, nm = b->count;
+    cudaError_t e = cudaSuccess;
+    for (int m = 0; m < nm && e == cudaSuccess; ++m)
+        e = cudaMemcpyAsync(b->lz[m].V, b->start[m], sizeof(double2) * b->lz[m].nc, cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return e;
+    mcpi::kb_reset<<<(nm + 127) / 128, 128, 0, st>>>(b->d_lz, nm, lm);
+    auto hpsi = [&](int vec) {
+        for (auto &G : b->groups) {
+            cudaError_t x = mcpi::launch_batch_apply_h(G.M, b->d_mem, G.w1, G.n1, G.sm1, G.w2, G.n2, G.sm2,
+                                                       vec, st);
+            if (x != cudaSuccess) return x;
+        }
+        return cudaSuccess;
+    };
+    const int nw = b->nvwork;
+    e = hpsi(0);
+    if (e != cudaSuccess) return e;
+    mcpi::kb_axpy_dot<<<nw, mcpi::kThreads, 0, st>>>(b->d_lz, b->d_vwork, -1);
+    mcpi::kb_sum_alpha<<<nm, mcpi::kThreads, 0, st>>>(b->d_lz, 0);
+    mcpi::kb_update<<<nw, mcpi::kThreads, 0, st>>>(b->d_lz, b->d_vwork, 0, 0);
+    for (int i = 0; i < lm - 1; ++i) {
+        mcpi::kb_beta<<<nm, mcpi::kThreads, 0, st>>>(b->d_lz, i, 1e-15);
+        mcpi::kb_scale<<<nw, mcpi::kThreads, 0, st>>>(b->d_lz, b->d_vwork, i);
+        e = hpsi(i + 1);
+        if (e != cudaSuccess) return e;
+        mcpi::kb_axpy_dot<<<nw, mcpi::kThreads, 0, st>>>(b->d_lz, b->d_vwork, i);
+        mcpi::kb_sum_alpha<<<nm, mcpi::kThreads, 0, st>>>(b->d_lz, i + 1);
+        mcpi::kb_multidot<<<nw, mcpi::kThreads, 0, st>>>(b->d_lz, b->d_vwork, i + 1, i + 2);
+        mcpi::kb_coef<<<nm, mcpi::kThreads, 0, st>>>(b->d_lz, i + 2);
+        mcpi::kb_update<<<nw, mcpi::kThreads, sizeof(double2) * (i + 2), st>>>(b->d_lz, b->d_vwork, i + 1,
+                                                                                 i + 2);
+    }
+    mcpi::kb_eig<<<(nm + 127) / 128, 128, 0, st>>>(b->d_lz, nm, b->d_E0, b->d_iters);
+    return cudaGetLastError();
+}
+
+int mcpi_batch_run(mcpi_batch b, double *h_E0, int *h_iters)
+{
+    if (!b) return bfail(MCPI_ERR_ARG, "null batch");
+    for (int m = 0; m < b->count; ++m)
+        if (b->ready[m] != 3) return bfail(MCPI_ERR_STATE, "every member needs integrals and a start vector");
+    if (cudaSetDevice(b->device) != cudaSuccess) return bfail(MCPI_ERR_CUDA, "cudaSetDevice failed");
+    cudaError_t e = cudaSuccess;
+    if (!b->exec) {
+        e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            cudaError_t q = enqueue_solve(b);
+            e = cudaStreamEndCapture(b->stream, &b->graph);
+            if (q != cudaSuccess) e = q;
+        }
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec, b->graph, 0);
+        if (e != cudaSuccess) return bfail(MCPI_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    }
+    e = cudaGraphLaunch(b->exec, b->stream);
+    if (e == cudaSuccess && h_E0)
+        e = cudaMemcpyAsync(h_E0, b->d_E0, sizeof(double) * b->count, cudaMemcpyDeviceToHost, b->stream);
+    if (e == cudaSuccess && h_iters)
+        e = cudaMemcpyAsync(h_iters, b->d_iters, sizeof(int) * b->count, cudaMemcpyDeviceToHost, b->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) return bfail(MCPI_ERR_CUDA, std::string("batch run: ") + cudaGetErrorString(e));
+    return MCPI_OK;
+}
+
+int mcpi_batch_arena_bytes(mcpi_batch b, size_t *bytes)
+{
+    if (!b || !bytes) return bfail(MCPI_ERR_ARG, "bad arguments");
+    *bytes = b->arena_bytes;
+    return MCPI_OK;
+}
+
+int mcpi_batch_destroy(mcpi_batch b)
+{
+    if (!b) return MCPI_OK;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    for (mcpi_space s : b->spaces) mcpi_space_destroy(s);
+    cudaFree(b->arena);
+    cudaFree(b->meta);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return MCPI_OK;
+}
+
+}  // extern "C"

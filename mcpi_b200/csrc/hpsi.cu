@@ -232,11 +232,10 @@ __global__ void __launch_bounds__(kT1b) k_pair_annihilate_blocks(Space sp, Space
 // hblk holds the blocks' dense values in that order (row-major per block).
 // ---------------------------------------------------------------------------
 template <int M>
-__global__ void __launch_bounds__(kT2, 3) k_pair_annihilate_momentum(Space sp, SpaceTables tb,
-                                                                  const double2 *__restrict__ hblk,
-                                                                  int nh,
-                                                                  const double2 *__restrict__ psi,
-                                                                  double2 *__restrict__ E)
+__device__ __forceinline__ void annihilate_momentum_body(const Space &sp, const SpaceTables &tb,
+                                                         const double2 *__restrict__ hblk, int nh,
+                                                         const double2 *__restrict__ psi,
+                                                         double2 *__restrict__ E, uint32_t block)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double2 *hv = reinterpret_cast<double2 *>(smem_raw);          // nh
@@ -246,7 +245,7 @@ __global__ void __launch_bounds__(kT2, 3) k_pair_annihilate_momentum(Space sp, S
     for (int x = threadIdx.x; x < nh; x += blockDim.x) hv[x] = hblk[x];
     __syncthreads();
 
-    const uint32_t m = blockIdx.x * kT2 + threadIdx.x;
+    const uint32_t m = block * kT2 + threadIdx.x;
     if (m >= sp.nc2) return;
     const int ws = sp.wstride;
     int u[M], Q[M];
@@ -293,6 +292,16 @@ __global__ void __launch_bounds__(kT2, 3) k_pair_annihilate_momentum(Space sp, S
             }
         off += n * n;
     }
+}
+
+template <int M>
+__global__ void __launch_bounds__(kT2, 3) k_pair_annihilate_momentum(Space sp, SpaceTables tb,
+                                                                  const double2 *__restrict__ hblk,
+                                                                  int nh,
+                                                                  const double2 *__restrict__ psi,
+                                                                  double2 *__restrict__ E)
+{
+    annihilate_momentum_body<M>(sp, tb, hblk, nh, psi, E, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -369,10 +378,11 @@ __global__ void __launch_bounds__(kT2, 4) k_pair_create(Space sp, SpaceTables tb
 // form; staging each block's contiguous E ranges in shared memory with TMA
 // bulk copies (0.73 ms) or prefetching them into L2 (0.28 ms) was slower.
 template <int M>
-__global__ void __launch_bounds__(kT2) k_pair_create_smem(Space sp, SpaceTables tb, PairOp op,
-                                                          const double2 *__restrict__ psi,
-                                                          const double2 *__restrict__ E,
-                                                          double2 *__restrict__ out)
+__device__ __forceinline__ void create_smem_body(const Space &sp, const SpaceTables &tb,
+                                                 const double2 *__restrict__ hdiag,
+                                                 const double2 *__restrict__ psi,
+                                                 const double2 *__restrict__ E,
+                                                 double2 *__restrict__ out, uint32_t block)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double *r1 = reinterpret_cast<double *>(smem_raw);             // M x kT2
@@ -383,11 +393,11 @@ __global__ void __launch_bounds__(kT2) k_pair_create_smem(Space sp, SpaceTables 
     double *sq = reinterpret_cast<double *>(hd + M);               // wstride
     uint32_t *W = reinterpret_cast<uint32_t *>(sq + sp.wstride);   // (M-1) x wstride
     load_tables(sp, tb, W, sq);
-    if (threadIdx.x < M) hd[threadIdx.x] = op.hdiag[threadIdx.x];
+    if (threadIdx.x < M) hd[threadIdx.x] = hdiag[threadIdx.x];
     __syncthreads();
 
     const int t = threadIdx.x;
-    const uint32_t i = blockIdx.x * kT2 + t;
+    const uint32_t i = block * kT2 + t;
     const bool row = i < sp.nc;
     const int ws = sp.wstride;
     double2 acc;
@@ -431,6 +441,62 @@ __global__ void __launch_bounds__(kT2) k_pair_create_smem(Space sp, SpaceTables 
             acc.y = fma(c, e.y, acc.y);
         }
     out[i] = acc;
+}
+
+template <int M>
+__global__ void __launch_bounds__(kT2) k_pair_create_smem(Space sp, SpaceTables tb, PairOp op,
+                                                          const double2 *__restrict__ psi,
+                                                          const double2 *__restrict__ E,
+                                                          double2 *__restrict__ out)
+{
+    create_smem_body<M>(sp, tb, op.hdiag, psi, E, out, blockIdx.x);
+}
+
+// ---------------------------------------------------------------------------
+// Batched H.psi: one launch applies H to the current Lanczos vector of every
+// member of a batch with the same M. A block's (member, block-in-member) pair
+// comes from a work table, so members of any size share the grid; members
+// whose Lanczos has stopped skip their blocks.
+// ---------------------------------------------------------------------------
+template <int M>
+__global__ void __launch_bounds__(kT2, 3) k_batch_annihilate(const BatchMember *__restrict__ mem,
+                                                          const int2 *__restrict__ work, int vec)
+{
+    const int2 w = work[blockIdx.x];
+    const BatchMember &b = mem[w.x];
+    if (*b.done) return;
+    annihilate_momentum_body<M>(b.sp, SpaceTables{b.W, b.sq}, b.hblk, b.nh,
+                                b.lvec + (size_t)vec * b.sp.nc, b.E, (uint32_t)w.y);
+}
+
+template <int M>
+__global__ void __launch_bounds__(kT2) k_batch_create(const BatchMember *__restrict__ mem,
+                                                      const int2 *__restrict__ work, int vec)
+{
+    const int2 w = work[blockIdx.x];
+    const BatchMember &b = mem[w.x];
+    if (*b.done) return;
+    create_smem_body<M>(b.sp, SpaceTables{b.W, b.sq}, b.hdiag, b.lvec + (size_t)vec * b.sp.nc, b.E,
+                        b.r, (uint32_t)w.y);
+}
+
+template <int M>
+cudaError_t batch_prepare_m(size_t smem1, size_t smem2)
+{
+    cudaError_t e = cudaFuncSetAttribute(k_batch_annihilate<M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem1);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_batch_create<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2);
+    return e;
+}
+
+template <int M>
+cudaError_t batch_apply_m(const BatchMember *mem, const int2 *work1, int n1, size_t smem1,
+                          const int2 *work2, int n2, size_t smem2, int vec, cudaStream_t st)
+{
+    if (n1) k_batch_annihilate<M><<<n1, kT2, smem1, st>>>(mem, work1, vec);
+    if (n2) k_batch_create<M><<<n2, kT2, smem2, st>>>(mem, work2, vec);
+    return cudaGetLastError();
 }
 
 // One particle: the configurations are the orbitals themselves (index(e_l) = l),
@@ -493,6 +559,43 @@ cudaError_t apply_h_m(const Space &sp, const SpaceTables &tb, const PairOp &op, 
 }
 
 }  // namespace
+
+cudaError_t launch_batch_apply_h(int M, const BatchMember *mem, const int2 *work1, int n1, size_t smem1,
+                                 const int2 *work2, int n2, size_t smem2, int vec, cudaStream_t st)
+{
+    switch (M) {
+#define MCPI_CASE(m) \
+    case m: return batch_apply_m<m>(mem, work1, n1, smem1, work2, n2, smem2, vec, st);
+        MCPI_CASE(2) MCPI_CASE(3) MCPI_CASE(4) MCPI_CASE(5) MCPI_CASE(6) MCPI_CASE(7) MCPI_CASE(8)
+        MCPI_CASE(9) MCPI_CASE(10) MCPI_CASE(11) MCPI_CASE(12) MCPI_CASE(13) MCPI_CASE(14)
+        MCPI_CASE(15) MCPI_CASE(16)
+#undef MCPI_CASE
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t batch_prepare(int M, size_t smem1, size_t smem2)
+{
+    switch (M) {
+#define MCPI_CASE(m) \
+    case m: return batch_prepare_m<m>(smem1, smem2);
+        MCPI_CASE(2) MCPI_CASE(3) MCPI_CASE(4) MCPI_CASE(5) MCPI_CASE(6) MCPI_CASE(7) MCPI_CASE(8)
+        MCPI_CASE(9) MCPI_CASE(10) MCPI_CASE(11) MCPI_CASE(12) MCPI_CASE(13) MCPI_CASE(14)
+        MCPI_CASE(15) MCPI_CASE(16)
+#undef MCPI_CASE
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+size_t batch_smem(int M, int N, int nh, int stage)
+{
+    const int ws = N + 3;
+    const size_t tab = sizeof(double) * ws + sizeof(uint32_t) * (M - 1) * ws;
+    if (stage == 1) return sizeof(double2) * nh + tab;
+    return (2 * sizeof(double) + 2 * sizeof(uint32_t)) * M * kT2 + sizeof(double2) * M + tab;
+}
+
+int batch_rows_per_block() { return kT2; }
 
 cudaError_t launch_apply_h(const Space &sp, const SpaceTables &tb, const PairOp &op,
                            const BlockOp &bo, const double2 *psi, double2 *E, double2 *out,

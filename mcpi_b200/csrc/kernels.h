@@ -54,6 +54,31 @@ cudaError_t launch_apply_h(const Space &sp, const SpaceTables &tb, const PairOp 
                            const BlockOp &bo, const double2 *psi, double2 *E, double2 *out,
                            cudaStream_t st, int stages = 3);
 
+// One member of a batched Lanczos, as the batched H.psi kernels see it
+// (momentum-block pair matrix only).
+struct BatchMember {
+    Space sp;
+    const uint32_t *W;
+    const double *sq;
+    const double2 *hblk;     // momentum-block pair matrix
+    int nh;
+    const double2 *hdiag;    // Ho[k][k]
+    const double2 *lvec;     // Krylov basis, vector k at lvec + k * nc
+    double2 *E;              // P x nc2 intermediate
+    double2 *r;              // H.psi output (the Lanczos residual)
+    const int *done;         // this member's breakdown flag
+};
+
+// Batched H.psi for the members of one M: work1 / work2 list (member,
+// block-in-member) for the annihilation / creation kernels; vec selects the
+// Krylov vector each member applies H to.
+cudaError_t launch_batch_apply_h(int M, const BatchMember *mem, const int2 *work1, int n1, size_t smem1,
+                                 const int2 *work2, int n2, size_t smem2, int vec, cudaStream_t st);
+size_t batch_smem(int M, int N, int nh, int stage);
+// Sets the kernels' shared-memory limits (call outside stream capture).
+cudaError_t batch_prepare(int M, size_t smem1, size_t smem2);
+int batch_rows_per_block();
+
 // Densities as Gram matrices over the (N-order)-particle space:
 // G[a][b] = sum_m conj(<m|A_a|phi>) <m|A_b|psi>, expanded to the reference
 // layouts: order 1 -> rho1[k*M + l]; order 2 -> rho2[k + s*M + q*M^2 + l*M^3].

@@ -1,0 +1,53 @@
+// Internal definition of the space context shared by the host-side
+// translation units (capi.cpp, batch.cu). Not part of the public ABI.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/mcpi_b200.h"
+#include "kernels.h"
+
+namespace mcpi {
+
+struct DevPairOp {
+    int *rowptr = nullptr;
+    uint16_t *col = nullptr;
+    double2 *val = nullptr;
+    double2 *hdiag = nullptr;
+    double2 *hfull = nullptr;
+    int nnz = 0;
+    int *prog = nullptr;       // block-sparse form (nullptr when a block is too wide)
+    int prog_bytes = 0;
+    double2 *hblk = nullptr;   // momentum-block form (nullptr when Ht couples different q+l)
+    int nhblk = 0;
+    int create_form = 0;
+    int *status = nullptr;     // the space's device status word (not owned)
+    PairOp view() const { return PairOp{rowptr, col, val, hdiag, hfull, nnz, hblk, nhblk, create_form, status}; }
+    BlockOp blocks() const { return BlockOp{prog, prog_bytes}; }
+};
+
+// Records msg as the calling thread's mcpi_last_error() and returns code.
+int set_error(int code, const char *msg);
+
+}  // namespace mcpi
+
+struct mcpi_space_s {
+    int N = 0, M = 0, device = 0;
+    mcpi::Space sp{};
+    int64_t nc = 0, nc1 = 0, nc2 = 0;
+    int P = 0;
+    cudaStream_t own = nullptr, stream = nullptr;
+    uint32_t *d_W = nullptr;
+    double *d_sq = nullptr;
+    bool has_op = false;
+    mcpi::DevPairOp fwd, adj;
+    double2 *d_E = nullptr;          // P * nc2 scratch of H.psi
+    double2 *d_gram = nullptr;       // density partials
+    size_t gram_cap = 0;
+    double2 *d_dot = nullptr;        // 1 result + partials
+    int *d_status = nullptr;         // device status word: 1 = a kernel's bounded wait timed out
+    bool dense_only = false;         // force the dense pair-matrix kernel
+    int kernel_choice = 0;           // 2: skip the momentum-block kernel
+    int create_form = 0;            // pair-creation kernel form (MCPI_OPT_CREATE_FORM)
+    mcpi::SpaceTables tables() const { return mcpi::SpaceTables{d_W, d_sq}; }
+};

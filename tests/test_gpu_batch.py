@@ -1,0 +1,62 @@
+"""Batched, graph-captured Lanczos ground states against the one-solve path.
+
+Every member must give the same lowest eigenvalue (|dE0| <= 1e-10, relative to
+max(1, |E0|)) and the same step count as mcpi_ground on the same start vector;
+a member that breaks down at once is masked while the others run on."""
+import numpy as np
+import pytest
+
+import mcpi_b200 as mc
+
+pytestmark = pytest.mark.gpu
+
+
+def _start(nc, seed):
+    rng = np.random.default_rng(seed)
+    C = rng.standard_normal(nc) + 1j * rng.standard_normal(nc)
+    return C / np.linalg.norm(C)
+
+
+def test_batch_matches_single_solves():
+    members = [(6, 7), (8, 9), (5, 11), (9, 7), (7, 9), (4, 11), (10, 7), (6, 9)]
+    gs = [0.05, 2.0, 30.0, 0.7, 11.0, 90.0, 0.01, 4.0]
+    lm = 40
+    b = mc.Batch(members, lm)
+    starts = []
+    for k, ((N, M), g) in enumerate(zip(members, gs)):
+        Ho, Hint = mc.lieb_integrals(M, g)
+        b.set_integrals(k, Ho, Hint)
+        C = _start(b.nc[k], 100 + k)
+        starts.append(C)
+        b.set_start(k, C)
+    E, it = b.run()
+    E2, it2 = b.run()          # replay of the captured graph gives the same answers
+    assert np.array_equal(E, E2) and np.array_equal(it, it2)
+    for k, ((N, M), g) in enumerate(zip(members, gs)):
+        sp = mc.FockSpace(N, M)
+        sp.set_integrals(*mc.lieb_integrals(M, g))
+        Es, _, its = sp.ground(starts[k], lm)
+        assert it[k] == its, (k, it[k], its)
+        assert abs(E[k] - Es) <= 1e-10 * max(1.0, abs(Es)), (k, E[k], Es)
+        sp.close()
+    b.close()
+
+
+def test_batch_masks_a_breakdown():
+    members = [(4, 5), (6, 7)]
+    b = mc.Batch(members, 20)
+    # member 0: all particles in the zero-momentum orbital of a free ring is an eigenvector
+    Ho, Hint = mc.lieb_integrals(5, 0.0)
+    b.set_integrals(0, Ho, Hint)
+    C0 = np.zeros(b.nc[0], np.complex128)
+    C0[mc.FockToIndex(4, 5, [0, 0, 4, 0, 0])] = 1.0
+    b.set_start(0, C0)
+    b.set_integrals(1, *mc.lieb_integrals(7, 3.0))
+    C1 = _start(b.nc[1], 7)
+    b.set_start(1, C1)
+    E, it = b.run()
+    assert it[0] == 0 and E[0] == pytest.approx(0.0, abs=1e-12)
+    sp = mc.FockSpace(6, 7)
+    sp.set_integrals(*mc.lieb_integrals(7, 3.0))
+    Es, _, its = sp.ground(C1, 20)
+    assert it[1] == its == 20 and abs(E[1] - Es) <= 1e-10 * abs(Es)
