@@ -155,6 +155,13 @@ MCPI_API int mcpi_lanczos(mcpi_space sp, void *d_lvec, int lm, double *h_diag, d
  * (groundStateLieb.c:348-471, ground). d_C receives the Ritz vector; *E0 the
  * eigenvalue. Allocates the niter*nc Krylov basis internally. */
 MCPI_API int mcpi_ground(mcpi_space sp, void *d_C, int niter, double *E0, int *iters);
+/* mcpi_ground for spaces whose niter x nc Krylov basis does not fit: plain
+ * three-term Lanczos (no reorthogonalisation; same breakdown rule) in two
+ * passes, the second regenerating the Krylov vectors -- bitwise the same, all
+ * reductions being deterministic -- to accumulate the Ritz vector. Holds four
+ * vectors of nc. Without reorthogonalisation the Lanczos matrix can acquire
+ * spurious copies of converged eigenvalues; the lowest one is unaffected. */
+MCPI_API int mcpi_ground_lowmem(mcpi_space sp, void *d_C, int niter, double *E0, int *iters);
 /* Eigenvalues (ascending, into d) and optionally row-major eigenvectors
  * z[k*n + j] of the symmetric tridiagonal (d, e): the LAPACKE_dstev('V') contract
  * used at groundStateLieb.c:435. Host arrays. */

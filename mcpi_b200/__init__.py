@@ -83,6 +83,7 @@ def lib():
         "mcpi_dot": (i, [_vp, _vp, _vp, _vp]),
         "mcpi_lanczos": (i, [_vp, _vp, i, _vp, _vp, pi]),
         "mcpi_ground": (i, [_vp, _vp, i, pd, pi]),
+        "mcpi_ground_lowmem": (i, [_vp, _vp, i, pd, pi]),
         "mcpi_tridiag_eig": (i, [i, _vp, _vp, _vp]),
         "mcpi_lieb_integrals": (i, [i, d, d, _vp, _vp]),
         "mcpi_batch_create": (i, [i, _vp, _vp, i, i, ct.POINTER(_vp)]),
@@ -345,13 +346,16 @@ class FockSpace:
                                   ct.byref(it)))
         return it.value, diag, off, lvec
 
-    def ground(self, C0, niter: int):
-        """groundStateLieb.c:348-471. Returns (E0, ground-state tensor, iterations)."""
+    def ground(self, C0, niter: int, lowmem: bool = False):
+        """groundStateLieb.c:348-471. Returns (E0, ground-state tensor, iterations).
+        lowmem: two-pass Lanczos that regenerates the Krylov vectors instead of
+        storing them (mcpi_ground_lowmem)."""
         C = self._vec(C0).clone()
         E = ct.c_double(0.0)
         it = ct.c_int(0)
         self._stream()
-        _check(lib().mcpi_ground(self._h, _vp(C.data_ptr()), niter, ct.byref(E), ct.byref(it)))
+        fn = lib().mcpi_ground_lowmem if lowmem else lib().mcpi_ground
+        _check(fn(self._h, _vp(C.data_ptr()), niter, ct.byref(E), ct.byref(it)))
         return E.value, C, it.value
 
 

@@ -866,6 +866,113 @@ int mcpi_ground(mcpi_space sp, void *d_C, int niter, double *E0, int *iters)
     return MCPI_OK;
 }
 
+// Two-pass Lanczos without reorthogonalisation, for spaces whose Krylov basis
+// does not fit: pass 1 keeps three vectors and records alpha/beta; pass 2
+// regenerates the same Krylov vectors from the stored alpha/beta (every kernel
+// and reduction is deterministic, so they are bitwise those of pass 1) and
+// accumulates the Ritz vector. Same breakdown rule as mcpi_lanczos.
+int mcpi_ground_lowmem(mcpi_space sp, void *d_C, int niter, double *E0, int *iters)
+{
+    CHECK_ARG(sp && d_C && E0 && niter >= 1 && niter <= 1 << 20, "mcpi_ground_lowmem: bad arguments");
+    if (!sp->has_op) return fail(MCPI_ERR_STATE, "mcpi_set_integrals has not been called");
+    DeviceGuard g(sp->device);
+    int rc = ensure_E(sp);
+    if (rc) return rc;
+    const int64_t nc = sp->nc;
+    const int lm = niter;
+    const size_t npart = mcpi::lanczos_partial_elems(nc, 1);
+    // state: alpha(lm) coef(lm) partial(npart) | beta(lm) maxbeta z(lm) | done iters
+    const size_t sbytes = sizeof(double2) * (2 * (size_t)lm + npart) + sizeof(double) * (2 * (size_t)lm + 1) +
+                          2 * sizeof(int);
+    char *blk = nullptr;
+    double2 *vec = nullptr;   // v[0], v[1], r, acc
+    CK(cudaMalloc(&blk, sbytes));
+    cudaError_t e = cudaMalloc(&vec, sizeof(double2) * nc * 4);
+    if (e != cudaSuccess) {
+        cudaFree(blk);
+        return fail(MCPI_ERR_NOMEM, "mcpi_ground_lowmem: %s", cudaGetErrorString(e));
+    }
+    mcpi::LanczosState s;
+    s.alpha = (double2 *)blk;
+    s.coef = s.alpha + lm;
+    s.partial = s.coef + lm;
+    s.beta = (double *)(s.partial + npart);
+    s.maxbeta = s.beta + lm;
+    double *dz = s.maxbeta + 1;
+    s.done = (int *)(dz + lm);
+    s.iters = s.done + 1;
+    s.nparts = mcpi::lanczos_parts(nc);
+    double2 *v[2] = {vec, vec + nc}, *r = vec + 2 * nc, *acc = vec + 3 * nc;
+    const PairOp op = sp->fwd.view();
+    const mcpi::BlockOp bo = sp->fwd.blocks();
+    const SpaceTables tb = sp->tables();
+    const int init[2] = {0, lm};
+    cudaStream_t st = sp->stream;
+    // pass 1: tridiagonal only
+    e = cudaMemsetAsync(blk, 0, sbytes, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(s.done, init, sizeof init, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(v[0], d_C, sizeof(double2) * nc, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = mcpi::launch_apply_h(sp->sp, tb, op, bo, v[0], sp->d_E, r, st);
+    if (e == cudaSuccess) e = mcpi::launch_lanczos_start(v[0], r, r, nc, s, st);
+    for (int i = 0; i < lm - 1 && e == cudaSuccess; ++i) {
+        double2 *vi = v[i & 1], *vn = v[(i + 1) & 1];
+        e = mcpi::launch_lanczos_beta(i, lm, 1e-15, s, st);
+        if (e == cudaSuccess) e = mcpi::launch_lanczos_scale(r, vn, nc, i, s, st);
+        if (e == cudaSuccess) e = mcpi::launch_apply_h(sp->sp, tb, op, bo, vn, sp->d_E, r, st);
+        if (e == cudaSuccess) e = mcpi::launch_lanczos_alpha(vi, vn, r, nc, i, s, st);
+        if (e == cudaSuccess) e = mcpi::launch_lanczos_no_reorth(vn, r, nc, i, s, st);
+    }
+    std::vector<double2> alpha(lm);
+    std::vector<double> beta(lm);
+    int it = lm;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(alpha.data(), s.alpha, sizeof(double2) * lm, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(beta.data(), s.beta, sizeof(double) * lm, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&it, s.iters, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    const int n = it > 0 ? it : 1;
+    std::vector<double> d(n), ee(n > 1 ? n - 1 : 1), z((size_t)n * n), zc(lm, 0.0);
+    int jmin = 0;
+    if (e == cudaSuccess) {
+        for (int k = 0; k < n; ++k) d[k] = alpha[k].x;
+        for (int k = 0; k + 1 < n; ++k) ee[k] = beta[k];
+        if (mcpi::tridiag_eig(n, d.data(), ee.data(), z.data()) != 0) {
+            cudaFree(blk);
+            cudaFree(vec);
+            return fail(MCPI_ERR_NUMERIC, "tridiagonal QL did not converge");
+        }
+        double sentinel = 1e10;
+        for (int k = 0; k < n; ++k)
+            if (sentinel > d[k]) {
+                sentinel = d[k];
+                jmin = k;
+            }
+        for (int k = 0; k < n; ++k) zc[k] = z[(size_t)k * n + jmin];
+    }
+    // pass 2: regenerate v_0 .. v_{n-1} and accumulate sum_k z_k v_k
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dz, zc.data(), sizeof(double) * lm, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(s.done, init, sizeof init, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(v[0], d_C, sizeof(double2) * nc, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = mcpi::launch_apply_h(sp->sp, tb, op, bo, v[0], sp->d_E, r, st);
+    if (e == cudaSuccess) e = mcpi::launch_lanczos_no_reorth(v[0], r, nc, -1, s, st);
+    if (e == cudaSuccess) e = mcpi::launch_axpy_real(acc, v[0], nc, dz, 1, st);
+    for (int i = 0; i < n - 1 && e == cudaSuccess; ++i) {
+        double2 *vi = v[i & 1], *vn = v[(i + 1) & 1];
+        e = mcpi::launch_lanczos_scale(r, vn, nc, i, s, st);
+        if (e == cudaSuccess) e = mcpi::launch_apply_h(sp->sp, tb, op, bo, vn, sp->d_E, r, st);
+        if (e == cudaSuccess) e = mcpi::launch_lanczos_axpy(vi, r, nc, i, s, st);
+        if (e == cudaSuccess) e = mcpi::launch_lanczos_no_reorth(vn, r, nc, i, s, st);
+        if (e == cudaSuccess) e = mcpi::launch_axpy_real(acc, vn, nc, dz + i + 1, 0, st);
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_C, acc, sizeof(double2) * nc, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(blk);
+    cudaFree(vec);
+    if (e != cudaSuccess) return fail(MCPI_ERR_CUDA, "mcpi_ground_lowmem: %s", cudaGetErrorString(e));
+    *E0 = d[jmin];
+    if (iters) *iters = it;
+    return check_status(sp);
+}
+
 int mcpi_lieb_integrals(int M, double g, double L, double *h_Ho, double *h_Hint)
 {
     CHECK_ARG(M >= 1 && h_Ho && h_Hint && L > 0, "mcpi_lieb_integrals: bad arguments");

@@ -128,6 +128,12 @@ cudaError_t launch_lanczos_reorth(const double2 *V, int nvec, double2 *r, int64_
                                   LanczosState s, cudaStream_t st);
 cudaError_t launch_combine(const double2 *V, int nvec, int64_t nc, const double *z,
                            double2 *out, cudaStream_t st);
+cudaError_t launch_lanczos_no_reorth(const double2 *vcur, double2 *r, int64_t nc, int i, LanczosState s,
+                                     cudaStream_t st);
+cudaError_t launch_axpy_real(double2 *acc, const double2 *v, int64_t nc, const double *z, int first,
+                             cudaStream_t st);
+cudaError_t launch_lanczos_axpy(const double2 *vprev, double2 *r, int64_t nc, int i, LanczosState s,
+                               cudaStream_t st);
 cudaError_t launch_dot(const double2 *a, const double2 *b, int64_t nc, double2 *partial,
                        double2 *result, cudaStream_t st);
 

@@ -119,6 +119,22 @@ __global__ void k_axpy_dot(const double2 *__restrict__ vprev, const double2 *__r
     if (threadIdx.x == 0) partial[blockIdx.x] = acc;
 }
 
+// r -= beta_i v_prev (the update of k_axpy_dot without its dot product)
+__global__ void k_axpy(const double2 *__restrict__ vprev, double2 *__restrict__ r, int64_t n,
+                       const double *beta_i, const int *done)
+{
+    if (stopped(done)) return;
+    const double b = *beta_i;
+    for (int64_t x = blockIdx.x * (int64_t)kThreads + threadIdx.x; x < n;
+         x += (int64_t)gridDim.x * kThreads) {
+        double2 y = r[x];
+        const double2 p = vprev[x];
+        y.x -= b * p.x;
+        y.y -= b * p.y;
+        r[x] = y;
+    }
+}
+
 // Pass 1: partial[j * nblk + b] = sum_{rows of slice b} conj(V_j) (r - alpha vcur)
 __global__ void __launch_bounds__(kThreads) k_multidot(const double2 *__restrict__ V, int nvec,
                                                        int64_t n, const double2 *__restrict__ r,
@@ -232,6 +248,22 @@ __global__ void k_scale(const double2 *__restrict__ r, double2 *__restrict__ vne
     }
 }
 
+// acc (+)= z * v, z real (read from device memory); first = 1 overwrites acc.
+__global__ void k_axpy_real(double2 *__restrict__ acc, const double2 *__restrict__ v, int64_t n,
+                            const double *z, int first, const int *done)
+{
+    if (stopped(done)) return;
+    const double c = *z;
+    for (int64_t x = blockIdx.x * (int64_t)kThreads + threadIdx.x; x < n;
+         x += (int64_t)gridDim.x * kThreads) {
+        const double2 p = v[x];
+        double2 a = first ? make_double2(0.0, 0.0) : acc[x];
+        a.x += p.x * c;
+        a.y += p.y * c;
+        acc[x] = a;
+    }
+}
+
 // out = sum_k V_k z_k (groundStateLieb.c:454-458), z real.
 __global__ void k_combine(const double2 *__restrict__ V, int nvec, int64_t n,
                           const double *__restrict__ z, double2 *__restrict__ out)
@@ -330,6 +362,29 @@ cudaError_t launch_lanczos_reorth(const double2 *V, int nvec, double2 *r, int64_
     const unsigned g = grid_for(nc);
     k_update<<<g, kThreads, sizeof(double2) * nvec, st>>>(V, nvec, nc, r, vcur, s.alpha + i + 1,
                                                          s.coef, s.partial, s.done);
+    return cudaGetLastError();
+}
+
+// r -= alpha_{i+1} v_{i+1} ; norm partials (the step without reorthogonalisation)
+cudaError_t launch_lanczos_no_reorth(const double2 *vcur, double2 *r, int64_t nc, int i, LanczosState s,
+                                     cudaStream_t st)
+{
+    k_update<<<grid_for(nc), kThreads, 0, st>>>(nullptr, 0, nc, r, vcur, s.alpha + i + 1, nullptr, s.partial,
+                                                s.done);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_lanczos_axpy(const double2 *vprev, double2 *r, int64_t nc, int i, LanczosState s,
+                               cudaStream_t st)
+{
+    k_axpy<<<grid_for(nc), kThreads, 0, st>>>(vprev, r, nc, s.beta + i, s.done);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_axpy_real(double2 *acc, const double2 *v, int64_t nc, const double *z, int first,
+                             cudaStream_t st)
+{
+    k_axpy_real<<<grid_for(nc), kThreads, 0, st>>>(acc, v, nc, z, first, nullptr);
     return cudaGetLastError();
 }
 
