@@ -54,6 +54,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-lanczos", action="store_true")
     p.add_argument("--no-batch", action="store_true")
+    p.add_argument("--no-large", action="store_true")
     return p.parse_args()
 
 
@@ -200,6 +201,49 @@ def run_batch(mc, torch, device, iters=120):
             "sequential_seconds": t_seq, "speedup_vs_sequential": t_seq / t_batch,
             "max_rel_dE0_vs_sequential": dE, "steps_done_min": int(it.min()),
             "nc_min": min(ncs), "nc_max": max(ncs), "arena_gb": arena / 1e9}
+
+
+def run_large(mc, torch, device):
+    """N=20, M=10 Lieb-Liniger at g=10 (nc = 10,015,005; 160 MB state): H.psi
+    throughput and HBM GB/s, 100 Lanczos steps, rho1 and rho2 of the result."""
+    N, M, g = 20, 10, 10.0
+    sp = mc.FockSpace(N, M, device=device)
+    sp.set_integrals(*mc.lieb_integrals(M, g, L_RING))
+    gen = torch.Generator(device=sp.torch_device)
+    gen.manual_seed(77)
+    x = torch.randn(sp.nc, dtype=torch.complex128, device=sp.torch_device, generator=gen)
+    x /= torch.linalg.vector_norm(x)
+    out = torch.empty_like(x)
+    for _ in range(3):
+        sp.apply_h(x, out)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(20):
+        sp.apply_h(x, out)
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / 20
+    byts = sum(hpsi_bytes(sp.nc, mc.nc_of(N - 2, M), sp.P).values())
+    t0 = time.perf_counter()
+    E0, psi, it = sp.ground(x, 100)
+    t_lz = time.perf_counter() - t0
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    r1 = sp.rho1(psi)
+    torch.cuda.synchronize()
+    t_r1 = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    r2 = sp.rho2(psi)
+    torch.cuda.synchronize()
+    t_r2 = time.perf_counter() - t0
+    occ = r1.diagonal().real.cpu().numpy()
+    sp.close()
+    return {"workload": "Lieb-Liniger N=20 M=10 g=10 (nc=10015005)", "hpsi_ms": ms,
+            "hpsi_per_s": 1e3 / ms, "hpsi_gbs": byts / (ms * 1e-3) / 1e9,
+            "lanczos_iterations": it, "E0": E0, "lanczos_seconds": t_lz,
+            "rho1_ms": 1e3 * t_r1, "rho2_ms": 1e3 * t_r2,
+            "occupations": [round(float(o), 6) for o in occ]}
 
 
 def cpu_setup(N, M, g):
@@ -405,6 +449,9 @@ def run_mcpi(args):
     batched = None
     if not args.no_batch:
         batched = run_batch(mc, torch, local)
+    large = None
+    if not args.no_large:
+        large = run_large(mc, torch, local)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -415,7 +462,8 @@ def run_mcpi(args):
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
                 "config": config(), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-                "gpu_launches": 2 * args.steps, "clocks": clk, "lanczos": lanczos, "batched": batched}
+                "gpu_launches": 2 * args.steps, "clocks": clk, "lanczos": lanczos, "batched": batched,
+                "large": large}
         print(json.dumps(line), flush=True)
     sp.close()
     if world > 1:
