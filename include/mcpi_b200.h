@@ -108,6 +108,10 @@ MCPI_API int mcpi_set_integrals(mcpi_space sp, const double *h_Ho, const double 
 /* out = H C (hamiltonianMatrix.h:891-1425 applyHconf_XX semantics; _omp, _X and
  * the CUDA applyHconf kernel compute the same; MCPI_VARIANT_HASH gives applyHconf). */
 MCPI_API int mcpi_apply_h(mcpi_space sp, const void *d_C, void *d_out);
+/* Rows [row0, row1) of H C into d_out[0 .. row1-row0), d_C being the whole
+ * vector: the local part of a row-sharded H.psi (each rank owns a row block
+ * and gathers the full vector first). Needs N >= 2. No reference counterpart. */
+MCPI_API int mcpi_apply_h_rows(mcpi_space sp, const void *d_C, int64_t row0, int64_t row1, void *d_out);
 /* mcpi_apply_h, timed: runs it reps times with CUDA events around each of its
  * two kernels on the space's stream (synchronising after every repetition) and
  * returns their mean durations in ms: h_ms[0] pair annihilation + pair-matrix

@@ -75,6 +75,7 @@ def lib():
         "mcpi_set_integrals": (i, [_vp, _vp, _vp, i]),
         "mcpi_apply_h": (i, [_vp, _vp, _vp]),
         "mcpi_apply_h_adjoint": (i, [_vp, _vp, _vp]),
+        "mcpi_apply_h_rows": (i, [_vp, _vp, i64, i64, _vp]),
         "mcpi_apply_h_profile": (i, [_vp, _vp, _vp, i, _vp]),
         "mcpi_rho1": (i, [_vp, _vp, _vp]),
         "mcpi_rho2": (i, [_vp, _vp, _vp]),
@@ -283,6 +284,15 @@ class FockSpace:
         out = self.empty() if out is None else out
         self._stream()
         _check(lib().mcpi_apply_h(self._h, _vp(C.data_ptr()), _vp(out.data_ptr())))
+        return out
+
+    def apply_h_rows(self, C, row0: int, row1: int, out=None):
+        """Rows [row0, row1) of H C (C the whole vector)."""
+        C = self._vec(C)
+        out = self.empty(row1 - row0) if out is None else out
+        self._stream()
+        _check(lib().mcpi_apply_h_rows(self._h, _vp(C.data_ptr()), row0, row1,
+                                       _vp(out.data_ptr()) if row1 > row0 else None))
         return out
 
     def apply_h_profile(self, C, out=None, reps: int = 10):

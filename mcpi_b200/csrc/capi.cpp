@@ -710,6 +710,23 @@ int mcpi_apply_h_profile(mcpi_space sp, const void *d_C, void *d_out, int reps, 
     return MCPI_OK;
 }
 
+int mcpi_apply_h_rows(mcpi_space sp, const void *d_C, int64_t row0, int64_t row1, void *d_out)
+{
+    CHECK_ARG(sp && d_C && d_C != d_out, "mcpi_apply_h_rows: bad arguments");
+    CHECK_ARG(row0 >= 0 && row0 <= row1 && row1 <= sp->nc, "mcpi_apply_h_rows: bad row range");
+    if (row0 == row1) return MCPI_OK;
+    CHECK_ARG(d_out, "mcpi_apply_h_rows: null output");
+    if (!sp->has_op) return fail(MCPI_ERR_STATE, "mcpi_set_integrals has not been called");
+    if (sp->N < 2 || sp->create_form != 0)
+        return fail(MCPI_ERR_ARG, "row ranges need N >= 2 and the default pair-creation form");
+    DeviceGuard g(sp->device);
+    int rc = ensure_E(sp);
+    if (rc) return rc;
+    CK(mcpi::launch_apply_h(sp->sp, sp->tables(), sp->fwd.view(), sp->fwd.blocks(), (const double2 *)d_C,
+                            sp->d_E, (double2 *)d_out, sp->stream, 3, (uint32_t)row0, (uint32_t)row1));
+    return MCPI_OK;
+}
+
 int mcpi_apply_h_adjoint(mcpi_space sp, const void *d_C, void *d_out)
 {
     return apply_op(sp, sp ? sp->adj : DevPairOp{}, d_C, d_out);

@@ -382,7 +382,8 @@ __device__ __forceinline__ void create_smem_body(const Space &sp, const SpaceTab
                                                  const double2 *__restrict__ hdiag,
                                                  const double2 *__restrict__ psi,
                                                  const double2 *__restrict__ E,
-                                                 double2 *__restrict__ out, uint32_t block)
+                                                 double2 *__restrict__ out, uint32_t block,
+                                                 uint32_t row0, uint32_t row1)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double *r1 = reinterpret_cast<double *>(smem_raw);             // M x kT2
@@ -397,8 +398,8 @@ __device__ __forceinline__ void create_smem_body(const Space &sp, const SpaceTab
     __syncthreads();
 
     const int t = threadIdx.x;
-    const uint32_t i = block * kT2 + t;
-    const bool row = i < sp.nc;
+    const uint32_t i = row0 + block * kT2 + t;   // rows [row0, row1) -> out[i - row0]
+    const bool row = i < row1;
     const int ws = sp.wstride;
     double2 acc;
     {
@@ -412,7 +413,7 @@ __device__ __forceinline__ void create_smem_body(const Space &sp, const SpaceTab
         }
         acc = row ? cmul(h1, psi[i]) : make_double2(0.0, 0.0);
         if (sp.N < 2) {
-            if (row) out[i] = acc;
+            if (row) out[i - row0] = acc;
             return;
         }
         uint32_t A0[M], Am1[M], Am2[M];
@@ -440,16 +441,17 @@ __device__ __forceinline__ void create_smem_body(const Space &sp, const SpaceTab
             acc.x = fma(c, e.x, acc.x);
             acc.y = fma(c, e.y, acc.y);
         }
-    out[i] = acc;
+    out[i - row0] = acc;
 }
 
 template <int M>
 __global__ void __launch_bounds__(kT2) k_pair_create_smem(Space sp, SpaceTables tb, PairOp op,
                                                           const double2 *__restrict__ psi,
                                                           const double2 *__restrict__ E,
-                                                          double2 *__restrict__ out)
+                                                          double2 *__restrict__ out, uint32_t row0,
+                                                          uint32_t row1)
 {
-    create_smem_body<M>(sp, tb, op.hdiag, psi, E, out, blockIdx.x);
+    create_smem_body<M>(sp, tb, op.hdiag, psi, E, out, blockIdx.x, row0, row1);
 }
 
 // ---------------------------------------------------------------------------
@@ -477,7 +479,7 @@ __global__ void __launch_bounds__(kT2) k_batch_create(const BatchMember *__restr
     const BatchMember &b = mem[w.x];
     if (*b.done) return;
     create_smem_body<M>(b.sp, SpaceTables{b.W, b.sq}, b.hdiag, b.lvec + (size_t)vec * b.sp.nc, b.E,
-                        b.r, (uint32_t)w.y);
+                        b.r, (uint32_t)w.y, 0u, b.sp.nc);
 }
 
 template <int M>
@@ -513,7 +515,8 @@ __global__ void k_one_particle(int M, const double2 *__restrict__ hfull,
 
 template <int M>
 cudaError_t apply_h_m(const Space &sp, const SpaceTables &tb, const PairOp &op, const BlockOp &bo,
-                      const double2 *psi, double2 *E, double2 *out, int stages, cudaStream_t st)
+                      const double2 *psi, double2 *E, double2 *out, int stages, cudaStream_t st,
+                      uint32_t row0, uint32_t row1)
 {
     constexpr int P = M * (M + 1) / 2;
     const size_t tab = sizeof(double) * sp.wstride + sizeof(uint32_t) * (M - 1) * sp.wstride;
@@ -548,9 +551,10 @@ cudaError_t apply_h_m(const Space &sp, const SpaceTables &tb, const PairOp &op, 
                 k_pair_create_smem<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2);
             if (e != cudaSuccess) return e;
         }
-        const unsigned g2 = (sp.nc + kT2 - 1) / kT2;
-        k_pair_create_smem<M><<<g2, kT2, sm2, st>>>(sp, tb, op, psi, E, out);
+        const unsigned g2 = (row1 - row0 + kT2 - 1) / kT2;
+        if (g2) k_pair_create_smem<M><<<g2, kT2, sm2, st>>>(sp, tb, op, psi, E, out, row0, row1);
     } else if (stages & 2) {
+        if (row0 != 0 || row1 != sp.nc) return cudaErrorInvalidValue;   // row ranges: shared-table form only
         const size_t sm2 = sizeof(double2) * M + tab;
         const unsigned g2 = (sp.nc + kT2 - 1) / kT2;
         k_pair_create<M><<<g2, kT2, sm2, st>>>(sp, tb, op, psi, E, out);
@@ -599,15 +603,18 @@ int batch_rows_per_block() { return kT2; }
 
 cudaError_t launch_apply_h(const Space &sp, const SpaceTables &tb, const PairOp &op,
                            const BlockOp &bo, const double2 *psi, double2 *E, double2 *out,
-                           cudaStream_t st, int stages)
+                           cudaStream_t st, int stages, uint32_t row0, uint32_t row1)
 {
+    if (row1 == 0xffffffffu) row1 = sp.nc;
+    if (row0 > row1 || row1 > sp.nc) return cudaErrorInvalidValue;
     if (sp.N == 1) {
+        if (row0 != 0 || row1 != sp.nc) return cudaErrorInvalidValue;
         if (stages & 2) k_one_particle<<<1, 32, 0, st>>>(sp.M, op.hfull, psi, out);
         return cudaGetLastError();
     }
     switch (sp.M) {
 #define MCPI_CASE(m) \
-    case m: return apply_h_m<m>(sp, tb, op, bo, psi, E, out, stages, st);
+    case m: return apply_h_m<m>(sp, tb, op, bo, psi, E, out, stages, st, row0, row1);
         MCPI_CASE(1) MCPI_CASE(2) MCPI_CASE(3) MCPI_CASE(4) MCPI_CASE(5) MCPI_CASE(6)
         MCPI_CASE(7) MCPI_CASE(8) MCPI_CASE(9) MCPI_CASE(10) MCPI_CASE(11) MCPI_CASE(12)
         MCPI_CASE(13) MCPI_CASE(14) MCPI_CASE(15) MCPI_CASE(16)

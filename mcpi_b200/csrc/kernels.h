@@ -50,9 +50,13 @@ struct SpaceTables {
 // H.psi : out = H psi. E is scratch of P * nc2 complex (unused when N < 2).
 // stages: bit 0 = kernel 1 (pair annihilation + pair matrix, writes E),
 //         bit 1 = kernel 2 (pair creation, reads E, writes out); 3 = both.
+// row0/row1: with the default shared-table creation kernel, only rows
+// [row0, row1) of out are computed, into out[0 .. row1-row0) (psi stays the
+// full vector); 0xffffffff = nc.
 cudaError_t launch_apply_h(const Space &sp, const SpaceTables &tb, const PairOp &op,
                            const BlockOp &bo, const double2 *psi, double2 *E, double2 *out,
-                           cudaStream_t st, int stages = 3);
+                           cudaStream_t st, int stages = 3, uint32_t row0 = 0,
+                           uint32_t row1 = 0xffffffffu);
 
 // One member of a batched Lanczos, as the batched H.psi kernels see it
 // (momentum-block pair matrix only).
