@@ -371,12 +371,15 @@ __global__ void __launch_bounds__(kT2, 4) k_pair_create(Space sp, SpaceTables tb
     out[i] = acc;
 }
 
-// Kernel 2, shared-table form (default): the per-row tables (Xr, Yr, sqrt v)
-// live in shared-memory columns that only their thread touches, so the pair
-// loop needs few registers (no spills) and the occupancy is set by shared
-// memory. Measured at N=16, M=10: 0.238 ms against 0.248 ms for the register
-// form; staging each block's contiguous E ranges in shared memory with TMA
-// bulk copies (0.73 ms) or prefetching them into L2 (0.28 ms) was slower.
+// Kernel 2, shared-table form (default): the per-row tables (Xr, Yr, sqrt v_k
+// and v_k - 1) live in shared-memory columns that only their thread touches,
+// so the pair loop needs few registers (no spills) and occupancy is set by
+// shared memory (17 bytes per orbital and row). Measured at N=16, M=10:
+// 0.198 ms, against 0.238 ms with two double tables, 0.248 ms for the register
+// form, 0.216 ms keeping only occupation bytes (square roots looked up per
+// pair), 0.21 ms forcing five blocks per SM (spills); staging each block's
+// contiguous E ranges in shared memory with TMA bulk copies (0.73 ms) or
+// prefetching them into L2 (0.28 ms) was slower still.
 template <int M>
 __device__ __forceinline__ void create_smem_body(const Space &sp, const SpaceTables &tb,
                                                  const double2 *__restrict__ hdiag,
@@ -387,10 +390,10 @@ __device__ __forceinline__ void create_smem_body(const Space &sp, const SpaceTab
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double *r1 = reinterpret_cast<double *>(smem_raw);             // M x kT2
-    double *r2 = r1 + M * kT2;                                     // M x kT2
-    uint32_t *Xr = reinterpret_cast<uint32_t *>(r2 + M * kT2);     // M x kT2
+    uint32_t *Xr = reinterpret_cast<uint32_t *>(r1 + M * kT2);     // M x kT2
     uint32_t *Yr = Xr + M * kT2;                                   // M x kT2
-    double2 *hd = reinterpret_cast<double2 *>(Yr + M * kT2);       // M
+    unsigned char *vb = reinterpret_cast<unsigned char *>(Yr + M * kT2);   // M x kT2
+    double2 *hd = reinterpret_cast<double2 *>(vb + ((M * kT2 + 15) & ~15)); // M
     double *sq = reinterpret_cast<double *>(hd + M);               // wstride
     uint32_t *W = reinterpret_cast<uint32_t *>(sq + sp.wstride);   // (M-1) x wstride
     load_tables(sp, tb, W, sq);
@@ -426,7 +429,7 @@ __device__ __forceinline__ void create_smem_body(const Space &sp, const SpaceTab
             Xr[o * kT2 + t] = base - (A0[o] - Am1[o]);
             Yr[o * kT2 + t] = Am1[o] - Am2[o];
             r1[o * kT2 + t] = row ? sq[v[o]] : 0.0;
-            r2[o * kT2 + t] = row ? sq[v[o]] * sq[v[o] >= 1 ? v[o] - 1 : 0] : 0.0;
+            vb[o * kT2 + t] = (unsigned char)(v[o] >= 1 ? v[o] - 1 : 0);
         }
     }
     const size_t stride = sp.nc2;
@@ -435,7 +438,7 @@ __device__ __forceinline__ void create_smem_body(const Space &sp, const SpaceTab
     for (int k = 0; k < M; ++k)
 #pragma unroll
         for (int s = k; s < M; ++s) {
-            const double c = (s == k) ? r2[k * kT2 + t] : r1[k * kT2 + t] * r1[s * kT2 + t];
+            const double c = r1[k * kT2 + t] * ((s == k) ? sq[vb[k * kT2 + t]] : r1[s * kT2 + t]);
             const uint32_t mm = c != 0.0 ? Xr[k * kT2 + t] - Yr[s * kT2 + t] : 0u;
             const double2 e = __ldg(E + pair_index(k, s, M) * stride + mm);
             acc.x = fma(c, e.x, acc.x);
@@ -545,7 +548,8 @@ cudaError_t apply_h_m(const Space &sp, const SpaceTables &tb, const PairOp &op, 
         k_pair_annihilate<M><<<g1, kT1, sm1, st>>>(sp, tb, op, psi, E);
     }
     if ((stages & 2) && sp.N >= 2 && op.create_form == 0) {
-        const size_t sm2 = (2 * sizeof(double) + 2 * sizeof(uint32_t)) * M * kT2 + sizeof(double2) * M + tab;
+        const size_t sm2 = (sizeof(double) + 2 * sizeof(uint32_t)) * M * kT2 + ((M * kT2 + 15) & ~15) +
+                           sizeof(double2) * M + tab;
         if (sm2 > 48 * 1024) {
             cudaError_t e = cudaFuncSetAttribute(
                 k_pair_create_smem<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2);
@@ -596,7 +600,8 @@ size_t batch_smem(int M, int N, int nh, int stage)
     const int ws = N + 3;
     const size_t tab = sizeof(double) * ws + sizeof(uint32_t) * (M - 1) * ws;
     if (stage == 1) return sizeof(double2) * nh + tab;
-    return (2 * sizeof(double) + 2 * sizeof(uint32_t)) * M * kT2 + sizeof(double2) * M + tab;
+    return (sizeof(double) + 2 * sizeof(uint32_t)) * M * kT2 + ((M * kT2 + 15) & ~15) + sizeof(double2) * M +
+           tab;
 }
 
 int batch_rows_per_block() { return kT2; }
