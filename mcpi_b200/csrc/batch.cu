@@ -410,13 +410,13 @@ int mcpi_batch_create(int count, const int *N, const int *M, int lm, int device,
     std::sort(Ms.begin(), Ms.end());
     Ms.erase(std::unique(Ms.begin(), Ms.end()), Ms.end());
     std::vector<std::vector<int2>> w1(Ms.size()), w2(Ms.size());
-    const int rpb = mcpi::batch_rows_per_block();
+    const int rpb1 = mcpi::batch_rows_per_block(1), rpb2 = mcpi::batch_rows_per_block(2);
     for (size_t g = 0; g < Ms.size(); ++g)
         for (int m = 0; m < count; ++m) {
             if (M[m] != Ms[g]) continue;
             const mcpi_space_s *s = b->spaces[m];
-            for (int64_t k = 0; k < (s->nc2 + rpb - 1) / rpb; ++k) w1[g].push_back(make_int2(m, (int)k));
-            for (int64_t k = 0; k < (s->nc + rpb - 1) / rpb; ++k) w2[g].push_back(make_int2(m, (int)k));
+            for (int64_t k = 0; k < (s->nc2 + rpb1 - 1) / rpb1; ++k) w1[g].push_back(make_int2(m, (int)k));
+            for (int64_t k = 0; k < (s->nc + rpb2 - 1) / rpb2; ++k) w2[g].push_back(make_int2(m, (int)k));
         }
     size_t mbytes = mcpi::up256(sizeof(BatchLz) * count) + mcpi::up256(sizeof(BatchMember) * count) +
                     mcpi::up256(sizeof(int2) * vwork.size()) + mcpi::up256(sizeof(double) * count) +

@@ -32,7 +32,8 @@ namespace {
 
 constexpr int kT1 = 64;    // threads (= (N-2)-configurations) per block, kernel 1
 constexpr int kCsrStaged = 1024;   // pair-matrix nonzeros staged in shared memory
-constexpr int kT2 = 256;   // threads per block, kernel 2
+constexpr int kT2 = 256;   // threads per block, kernel 2 (register form) and kernel 1 (momentum form)
+constexpr int kTC = 256;   // threads (= rows) per block, kernel 2 (shared-table form)
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
 {
@@ -389,11 +390,11 @@ __device__ __forceinline__ void create_smem_body(const Space &sp, const SpaceTab
                                                  uint32_t row0, uint32_t row1)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    double *r1 = reinterpret_cast<double *>(smem_raw);             // M x kT2
-    uint32_t *Xr = reinterpret_cast<uint32_t *>(r1 + M * kT2);     // M x kT2
-    uint32_t *Yr = Xr + M * kT2;                                   // M x kT2
-    unsigned char *vb = reinterpret_cast<unsigned char *>(Yr + M * kT2);   // M x kT2
-    double2 *hd = reinterpret_cast<double2 *>(vb + ((M * kT2 + 15) & ~15)); // M
+    double *r1 = reinterpret_cast<double *>(smem_raw);             // M x kTC
+    uint32_t *Xr = reinterpret_cast<uint32_t *>(r1 + M * kTC);     // M x kTC
+    uint32_t *Yr = Xr + M * kTC;                                   // M x kTC
+    unsigned char *vb = reinterpret_cast<unsigned char *>(Yr + M * kTC);   // M x kTC
+    double2 *hd = reinterpret_cast<double2 *>(vb + ((M * kTC + 15) & ~15)); // M
     double *sq = reinterpret_cast<double *>(hd + M);               // wstride
     uint32_t *W = reinterpret_cast<uint32_t *>(sq + sp.wstride);   // (M-1) x wstride
     load_tables(sp, tb, W, sq);
@@ -401,7 +402,7 @@ __device__ __forceinline__ void create_smem_body(const Space &sp, const SpaceTab
     __syncthreads();
 
     const int t = threadIdx.x;
-    const uint32_t i = row0 + block * kT2 + t;   // rows [row0, row1) -> out[i - row0]
+    const uint32_t i = row0 + block * kTC + t;   // rows [row0, row1) -> out[i - row0]
     const bool row = i < row1;
     const int ws = sp.wstride;
     double2 acc;
@@ -426,10 +427,10 @@ __device__ __forceinline__ void create_smem_body(const Space &sp, const SpaceTab
         const uint32_t base = sp.nc2 - 1u - Am2[M - 1];
 #pragma unroll
         for (int o = 0; o < M; ++o) {
-            Xr[o * kT2 + t] = base - (A0[o] - Am1[o]);
-            Yr[o * kT2 + t] = Am1[o] - Am2[o];
-            r1[o * kT2 + t] = row ? sq[v[o]] : 0.0;
-            vb[o * kT2 + t] = (unsigned char)(v[o] >= 1 ? v[o] - 1 : 0);
+            Xr[o * kTC + t] = base - (A0[o] - Am1[o]);
+            Yr[o * kTC + t] = Am1[o] - Am2[o];
+            r1[o * kTC + t] = row ? sq[v[o]] : 0.0;
+            vb[o * kTC + t] = (unsigned char)(v[o] >= 1 ? v[o] - 1 : 0);
         }
     }
     const size_t stride = sp.nc2;
@@ -438,8 +439,8 @@ __device__ __forceinline__ void create_smem_body(const Space &sp, const SpaceTab
     for (int k = 0; k < M; ++k)
 #pragma unroll
         for (int s = k; s < M; ++s) {
-            const double c = r1[k * kT2 + t] * ((s == k) ? sq[vb[k * kT2 + t]] : r1[s * kT2 + t]);
-            const uint32_t mm = c != 0.0 ? Xr[k * kT2 + t] - Yr[s * kT2 + t] : 0u;
+            const double c = r1[k * kTC + t] * ((s == k) ? sq[vb[k * kTC + t]] : r1[s * kTC + t]);
+            const uint32_t mm = c != 0.0 ? Xr[k * kTC + t] - Yr[s * kTC + t] : 0u;
             const double2 e = __ldg(E + pair_index(k, s, M) * stride + mm);
             acc.x = fma(c, e.x, acc.x);
             acc.y = fma(c, e.y, acc.y);
@@ -448,7 +449,7 @@ __device__ __forceinline__ void create_smem_body(const Space &sp, const SpaceTab
 }
 
 template <int M>
-__global__ void __launch_bounds__(kT2) k_pair_create_smem(Space sp, SpaceTables tb, PairOp op,
+__global__ void __launch_bounds__(kTC) k_pair_create_smem(Space sp, SpaceTables tb, PairOp op,
                                                           const double2 *__restrict__ psi,
                                                           const double2 *__restrict__ E,
                                                           double2 *__restrict__ out, uint32_t row0,
@@ -475,7 +476,7 @@ __global__ void __launch_bounds__(kT2, 3) k_batch_annihilate(const BatchMember *
 }
 
 template <int M>
-__global__ void __launch_bounds__(kT2) k_batch_create(const BatchMember *__restrict__ mem,
+__global__ void __launch_bounds__(kTC) k_batch_create(const BatchMember *__restrict__ mem,
                                                       const int2 *__restrict__ work, int vec)
 {
     const int2 w = work[blockIdx.x];
@@ -500,7 +501,7 @@ cudaError_t batch_apply_m(const BatchMember *mem, const int2 *work1, int n1, siz
                           const int2 *work2, int n2, size_t smem2, int vec, cudaStream_t st)
 {
     if (n1) k_batch_annihilate<M><<<n1, kT2, smem1, st>>>(mem, work1, vec);
-    if (n2) k_batch_create<M><<<n2, kT2, smem2, st>>>(mem, work2, vec);
+    if (n2) k_batch_create<M><<<n2, kTC, smem2, st>>>(mem, work2, vec);
     return cudaGetLastError();
 }
 
@@ -548,15 +549,15 @@ cudaError_t apply_h_m(const Space &sp, const SpaceTables &tb, const PairOp &op, 
         k_pair_annihilate<M><<<g1, kT1, sm1, st>>>(sp, tb, op, psi, E);
     }
     if ((stages & 2) && sp.N >= 2 && op.create_form == 0) {
-        const size_t sm2 = (sizeof(double) + 2 * sizeof(uint32_t)) * M * kT2 + ((M * kT2 + 15) & ~15) +
+        const size_t sm2 = (sizeof(double) + 2 * sizeof(uint32_t)) * M * kTC + ((M * kTC + 15) & ~15) +
                            sizeof(double2) * M + tab;
         if (sm2 > 48 * 1024) {
             cudaError_t e = cudaFuncSetAttribute(
                 k_pair_create_smem<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2);
             if (e != cudaSuccess) return e;
         }
-        const unsigned g2 = (row1 - row0 + kT2 - 1) / kT2;
-        if (g2) k_pair_create_smem<M><<<g2, kT2, sm2, st>>>(sp, tb, op, psi, E, out, row0, row1);
+        const unsigned g2 = (row1 - row0 + kTC - 1) / kTC;
+        if (g2) k_pair_create_smem<M><<<g2, kTC, sm2, st>>>(sp, tb, op, psi, E, out, row0, row1);
     } else if (stages & 2) {
         if (row0 != 0 || row1 != sp.nc) return cudaErrorInvalidValue;   // row ranges: shared-table form only
         const size_t sm2 = sizeof(double2) * M + tab;
@@ -600,11 +601,11 @@ size_t batch_smem(int M, int N, int nh, int stage)
     const int ws = N + 3;
     const size_t tab = sizeof(double) * ws + sizeof(uint32_t) * (M - 1) * ws;
     if (stage == 1) return sizeof(double2) * nh + tab;
-    return (sizeof(double) + 2 * sizeof(uint32_t)) * M * kT2 + ((M * kT2 + 15) & ~15) + sizeof(double2) * M +
+    return (sizeof(double) + 2 * sizeof(uint32_t)) * M * kTC + ((M * kTC + 15) & ~15) + sizeof(double2) * M +
            tab;
 }
 
-int batch_rows_per_block() { return kT2; }
+int batch_rows_per_block(int stage) { return stage == 1 ? kT2 : kTC; }
 
 cudaError_t launch_apply_h(const Space &sp, const SpaceTables &tb, const PairOp &op,
                            const BlockOp &bo, const double2 *psi, double2 *E, double2 *out,

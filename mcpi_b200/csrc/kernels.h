@@ -81,7 +81,8 @@ cudaError_t launch_batch_apply_h(int M, const BatchMember *mem, const int2 *work
 size_t batch_smem(int M, int N, int nh, int stage);
 // Sets the kernels' shared-memory limits (call outside stream capture).
 cudaError_t batch_prepare(int M, size_t smem1, size_t smem2);
-int batch_rows_per_block();
+// configurations per block of the batched kernels: stage 1 annihilation, 2 creation
+int batch_rows_per_block(int stage);
 
 // Densities as Gram matrices over the (N-order)-particle space:
 // G[a][b] = sum_m conj(<m|A_a|phi>) <m|A_b|psi>, expanded to the reference
