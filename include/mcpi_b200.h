@@ -59,7 +59,7 @@ MCPI_API int mcpi_space_destroy(mcpi_space sp);
  * legacy default stream). A new space uses a private non-blocking stream. */
 MCPI_API int mcpi_space_set_stream(mcpi_space sp, void *stream);
 MCPI_API int mcpi_space_sync(mcpi_space sp);
-/* Space options. MCPI_OPT_DENSE_PAIR_KERNEL (value 0/1): always use the dense
+/* Space options. MCPI_OPT_DENSE_PAIR_KERNEL (value 0/1): always use a dense
  * pair-matrix kernel for H.psi even when the integrals decompose into small
  * blocks (takes effect at the next mcpi_set_integrals). */
 #define MCPI_OPT_DENSE_PAIR_KERNEL 1
@@ -71,6 +71,10 @@ MCPI_API int mcpi_space_sync(mcpi_space sp);
  * tables in shared memory (default), 1 per-row tables in registers. Takes
  * effect at the next mcpi_set_integrals. */
 #define MCPI_OPT_CREATE_FORM 3
+/* MCPI_OPT_NO_GEMM_KERNEL (0/1): general (dense) pair matrices use the
+ * compressed-row kernel instead of the register-tiled dense product (which is
+ * otherwise chosen for M <= 12). Takes effect at the next mcpi_set_integrals. */
+#define MCPI_OPT_NO_GEMM_KERNEL 4
 MCPI_API int mcpi_space_set_option(mcpi_space sp, int option, int value);
 MCPI_API int mcpi_space_dims(mcpi_space sp, int *N, int *M, int64_t *nc);
 /* Device memory on the space's device, and a synchronous copy in any direction

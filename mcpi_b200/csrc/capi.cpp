@@ -100,6 +100,7 @@ void free_op(DevPairOp &o)
     cudaFree(o.val);
     cudaFree(o.hdiag);
     cudaFree(o.hfull);
+    cudaFree(o.hdense);
     o = DevPairOp{};
 }
 
@@ -284,6 +285,14 @@ int upload_op(mcpi_space_s *sp, DevPairOp &op, const std::vector<cplx> &Ht, cons
         CK(cudaMemcpyAsync(op.prog, prog.data(), sizeof(int) * prog.size(), cudaMemcpyHostToDevice, sp->stream));
         op.prog_bytes = (int)(sizeof(int) * prog.size());
     }
+    // General pair matrices: the register-tiled product does P^2 complex
+    // multiply-adds per (N-2)-configuration at full FP64 rate, the CSR form
+    // nnz at a fraction of it, so the dense form pays once a quarter is filled.
+    const bool general = (mom.empty() || sp->kernel_choice == 2) && prog.empty() && 4 * col.size() >= (size_t)P * P;
+    if (P <= mcpi::kGemmMaxP && !sp->no_gemm && (sp->dense_only || general)) {
+        CK(cudaMalloc(&op.hdense, sizeof(double2) * P * P));
+        CK(cudaMemcpyAsync(op.hdense, Ht.data(), sizeof(double2) * P * P, cudaMemcpyHostToDevice, sp->stream));
+    }
     CK(cudaStreamSynchronize(sp->stream));  // host vectors go out of scope
     op.nnz = (int)col.size();
     return MCPI_OK;
@@ -455,6 +464,7 @@ int mcpi_space_set_option(mcpi_space sp, int option, int value)
     switch (option) {
     case MCPI_OPT_DENSE_PAIR_KERNEL: sp->dense_only = value != 0; return MCPI_OK;
     case MCPI_OPT_NO_MOMENTUM_KERNEL: sp->kernel_choice = value ? 2 : 0; return MCPI_OK;
+    case MCPI_OPT_NO_GEMM_KERNEL: sp->no_gemm = value != 0; return MCPI_OK;
     case MCPI_OPT_CREATE_FORM:
         sp->create_form = value;
         sp->fwd.create_form = sp->adj.create_form = value;

@@ -141,6 +141,104 @@ __global__ void __launch_bounds__(kT1) k_pair_annihilate(Space sp, SpaceTables t
 }
 
 // ---------------------------------------------------------------------------
+// kernel 1, dense-product form for general pair matrices (P <= kGemmMaxP).
+// A persistent block keeps Ht (P x P, zero-padded to PA = 8 * RA rows) in
+// shared memory. Per tile of kGM (N-2)-configurations it gathers
+// D[b][m] = c_b(m) psi[index(m + pair b)] into shared memory (kTG / kGM threads
+// per configuration, cp.async), then forms E[a][m] = sum_b Ht[a][b] D[b][m] as a
+// register-tiled complex FP64 product: warp w owns the rows a = w*RA .. w*RA+RA-1
+// (Ht reads are warp-uniform broadcasts), lane owns the columns m = lane and
+// lane + 32 (conflict-free 16-byte reads of D, coalesced evict-first stores of E).
+// Per configuration: P gathers, 4 P^2 FP64 FMAs, P stores.
+// ---------------------------------------------------------------------------
+constexpr int kTG = 256;   // threads per block, dense-product form
+constexpr int kGM = 64;    // (N-2)-configurations per tile
+
+template <int M>
+__global__ void __launch_bounds__(kTG, M <= 10 ? 2 : 1) k_pair_annihilate_gemm(Space sp, SpaceTables tb,
+                                                                 const double2 *__restrict__ H,
+                                                                 const double2 *__restrict__ psi,
+                                                                 double2 *__restrict__ E, uint32_t ntiles)
+{
+    constexpr int P = M * (M + 1) / 2;
+    constexpr int RA = (P + 7) / 8;
+    constexpr int PA = 8 * RA;
+    constexpr int kParts = kTG / kGM;
+    static_assert(kTG == 256 && kGM == 64, "8 warps x RA rows, 2 columns per lane");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2 *Hs = reinterpret_cast<double2 *>(smem_raw);          // PA x P
+    double2 *D = Hs + PA * P;                                     // P x kGM
+    double *sq = reinterpret_cast<double *>(D + P * kGM);
+    uint32_t *W = reinterpret_cast<uint32_t *>(sq + sp.wstride);
+    load_tables(sp, tb, W, sq);
+    for (int x = threadIdx.x; x < PA * P; x += kTG) Hs[x] = x < P * P ? H[x] : make_double2(0.0, 0.0);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int cfg = threadIdx.x % kGM, part = threadIdx.x / kGM;
+    const int ws = sp.wstride;
+    const size_t stride = sp.nc2;
+    const double2 *Hw = Hs + warp * RA * P;
+    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const uint32_t m0 = tile * kGM;
+        const uint32_t m = m0 + cfg;
+        __syncthreads();   // tables loaded (first tile) / previous tile's D consumed
+        if (m < sp.nc2) {
+            int u[M], Q[M];
+            decode<M>(m, sp.N - 2, sp.nc2, W, ws, u, Q);
+            uint32_t B0[M], B1[M], B2[M];
+            prefix_table<M>(Q, 0, W, ws, B0);
+            prefix_table<M>(Q, 1, W, ws, B1);
+            prefix_table<M>(Q, 2, W, ws, B2);
+#pragma unroll
+            for (int q = 0; q < M; ++q)
+#pragma unroll
+                for (int l = q; l < M; ++l)
+                    if (pair_index(q, l, M) % kParts == part) {
+                        const uint32_t j = idx_add2(sp.nc, B0, B1, B2, q, l, M);
+                        cp_async16(D + pair_index(q, l, M) * kGM + cfg, psi + j);
+                    }
+            cp_async_wait_all();
+#pragma unroll
+            for (int q = 0; q < M; ++q)
+#pragma unroll
+                for (int l = q; l < M; ++l)
+                    if (pair_index(q, l, M) % kParts == part) {
+                        const double c = (q == l) ? sq[u[q] + 1] * sq[u[q] + 2] : sq[u[q] + 1] * sq[u[l] + 1];
+                        double2 &d = D[pair_index(q, l, M) * kGM + cfg];
+                        d.x *= c;
+                        d.y *= c;
+                    }
+        } else {
+            for (int b = part; b < P; b += kParts) D[b * kGM + cfg] = make_double2(0.0, 0.0);
+        }
+        __syncthreads();
+
+        double2 acc0[RA], acc1[RA];
+#pragma unroll
+        for (int i = 0; i < RA; ++i) acc0[i] = acc1[i] = make_double2(0.0, 0.0);
+#pragma unroll 5
+        for (int k = 0; k < P; ++k) {
+            const double2 d0 = D[k * kGM + lane], d1 = D[k * kGM + lane + 32];
+#pragma unroll
+            for (int i = 0; i < RA; ++i) {
+                const double2 h = Hw[i * P + k];
+                cfma(acc0[i], h, d0);
+                cfma(acc1[i], h, d1);
+            }
+        }
+        const bool ok0 = m0 + lane < sp.nc2, ok1 = m0 + lane + 32 < sp.nc2;
+#pragma unroll
+        for (int i = 0; i < RA; ++i) {
+            const int a = warp * RA + i;
+            if (a < P) {
+                if (ok0) __stcs(E + a * stride + m0 + lane, acc0[i]);
+                if (ok1) __stcs(E + a * stride + m0 + lane + 32, acc1[i]);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // kernel 1, block-sparse form: the same E, one pair-matrix block at a time.
 // Each thread keeps, per orbital t, X[t] = B0[t]-B1[t], Y[t] = B1[t]-B2[t]
 // (so index(m + e_q + e_l) = nc - 1 - (X[q] + Y[l] + B2[M-1]), q <= l) and the
@@ -537,6 +635,20 @@ cudaError_t apply_h_m(const Space &sp, const SpaceTables &tb, const PairOp &op, 
         }
         const unsigned g1 = (sp.nc2 + kT1b - 1) / kT1b;
         k_pair_annihilate_blocks<M><<<g1, kT1b, smb, st>>>(sp, tb, bo, psi, E);
+    } else if (sp.N >= 2 && (stages & 1) && op.hdense && P <= kGemmMaxP) {
+        if constexpr (P <= kGemmMaxP) {
+            constexpr int PA = 8 * ((P + 7) / 8);
+            const size_t smg = sizeof(double2) * (PA * P + P * kGM) + tab;
+            cudaError_t e = cudaFuncSetAttribute(k_pair_annihilate_gemm<M>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smg);
+            if (e != cudaSuccess) return e;
+            int dev = 0, sms = 0;
+            if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+            if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+            const uint32_t ntiles = (uint32_t)((sp.nc2 + kGM - 1) / kGM);
+            const unsigned g1 = ntiles < 2u * sms ? ntiles : 2u * sms;
+            if (g1) k_pair_annihilate_gemm<M><<<g1, kTG, smg, st>>>(sp, tb, op.hdense, psi, E, ntiles);
+        }
     } else if (sp.N >= 2 && (stages & 1)) {
         const int st_nnz = op.nnz <= kCsrStaged ? op.nnz : 0;
         const size_t sm1 = sizeof(double2) * (P * kT1 + st_nnz) + tab + sizeof(int) * (P + 1 + st_nnz);

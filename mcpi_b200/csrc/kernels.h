@@ -25,7 +25,11 @@ struct PairOp {
     int nhblk;
     int create_form;        // pair-creation kernel: 0 per-row tables in shared memory, 1 in registers
     int *status;            // device status word (1: a bounded wait timed out)
+    // dense form (nullptr unless set): Ht as P x P row-major, for pair matrices with
+    // no momentum-block or narrow block structure and P <= kGemmMaxP
+    const double2 *hdense;
 };
+constexpr int kGemmMaxP = 78;   // M <= 12: Ht (zero-padded to a multiple of 8 rows) fits shared memory
 
 // Block-sparse form of the same pair matrix: when Ht decomposes into blocks
 // (rows R_b x columns C_b, e.g. one block per total momentum for plane-wave

@@ -22,7 +22,11 @@ struct DevPairOp {
     int nhblk = 0;
     int create_form = 0;
     int *status = nullptr;     // the space's device status word (not owned)
-    PairOp view() const { return PairOp{rowptr, col, val, hdiag, hfull, nnz, hblk, nhblk, create_form, status}; }
+    double2 *hdense = nullptr; // dense form (nullptr unless Ht is general and P <= kGemmMaxP)
+    PairOp view() const
+    {
+        return PairOp{rowptr, col, val, hdiag, hfull, nnz, hblk, nhblk, create_form, status, hdense};
+    }
     BlockOp blocks() const { return BlockOp{prog, prog_bytes}; }
 };
 
@@ -48,6 +52,7 @@ struct mcpi_space_s {
     int *d_status = nullptr;         // device status word: 1 = a kernel's bounded wait timed out
     bool dense_only = false;         // force the dense pair-matrix kernel
     int kernel_choice = 0;           // 2: skip the momentum-block kernel
+    bool no_gemm = false;            // general pair matrices use the CSR kernel (MCPI_OPT_NO_GEMM_KERNEL)
     int create_form = 0;            // pair-creation kernel form (MCPI_OPT_CREATE_FORM)
     mcpi::SpaceTables tables() const { return mcpi::SpaceTables{d_W, d_sq}; }
 };

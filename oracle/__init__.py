@@ -40,6 +40,8 @@ def build(ref: bool = True) -> None:
     targets = ["liborc.so"]
     if ref and os.path.exists(os.path.join(REFERENCE_SRC, "configurationsMap.h")):
         targets.append("ref")
+        if os.path.exists(os.path.join(REFERENCE_SRC, "cuda", "hamiltonianMatrix.cuh")):
+            targets.append("refcuda")
         if os.path.exists(os.path.join(HERE, "..", "mcpi_b200", "libmcpi_dropin.so")):
             targets.append("dropin")
     subprocess.run(["make", "-s", "-C", HERE, f"REF={REFERENCE_SRC}", *targets], check=True)
@@ -441,3 +443,68 @@ class Ref:
                             _ptr(t["Map"]), _ptr(t["MapOT"]), _ptr(t["MapTT"]), hp,
                             _ptr(np.ascontiguousarray(Hint, np.complex128)), _ptr(C))
         return E, C
+
+
+# ---------------------------------------------------------------------------
+# the reference's own CUDA kernel (cuda/hamiltonianMatrix.cuh:60-626)
+# ---------------------------------------------------------------------------
+REFCUDA_PATH = os.path.join(HERE, "_ref", "libmcpi_refcuda.so")
+REFCUDA_HOST_PATH = os.path.join(HERE, "_ref", "refcuda_host")
+
+
+def refcuda_available() -> bool:
+    return os.path.exists(REFCUDA_PATH) and os.path.exists(REFCUDA_HOST_PATH)
+
+
+def _cuda_layout(Ho):
+    # the kernel reads Ho[k + M*l] for the CPU reference's Ho[k][l]
+    return np.ascontiguousarray(np.asarray(Ho, np.complex128).T)
+
+
+def refcuda_host_apply_h(N, M, C, Ho, Hint, workdir):
+    """H C from the reference CUDA kernel's source run on the host under
+    AddressSanitizer (oracle/refcuda_host.cpp). Raises on any sanitizer report."""
+    inp = os.path.join(workdir, f"refcuda_in_{N}_{M}.bin")
+    outp = os.path.join(workdir, f"refcuda_out_{N}_{M}.bin")
+    with open(inp, "wb") as f:
+        f.write(np.ascontiguousarray(C, np.complex128).tobytes())
+        f.write(_cuda_layout(Ho).tobytes())
+        f.write(np.ascontiguousarray(Hint, np.complex128).tobytes())
+    env = dict(os.environ, ASAN_OPTIONS="detect_leaks=0:halt_on_error=1:abort_on_error=0")
+    r = subprocess.run([REFCUDA_HOST_PATH, str(N), str(M), inp, outp], env=env,
+                       capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"refcuda_host N={N} M={M} failed ({r.returncode}):\n{r.stderr[-4000:]}")
+    return np.fromfile(outp, np.complex128)
+
+
+class RefCuda:
+    """ctypes view of oracle/_ref/libmcpi_refcuda.so: the reference CUDA kernel
+    with its own int32 maps, launched as cuda/performanceTest.cu launches it."""
+
+    def __init__(self, path: str = REFCUDA_PATH):
+        L = ct.CDLL(path)
+        L.refcuda_fits.restype = ct.c_int
+        L.refcuda_fits.argtypes = [ct.c_int, ct.c_int]
+        L.refcuda_map_bytes.restype = ct.c_int64
+        L.refcuda_apply_h.restype = ct.c_int
+        L.refcuda_apply_h.argtypes = [ct.c_int, ct.c_int, _vp, _vp, _vp, _vp, ct.c_int,
+                                      ct.POINTER(ct.c_float), ct.c_char_p, ct.c_int]
+        self.lib = L
+
+    def fits(self, N, M) -> bool:
+        return bool(self.lib.refcuda_fits(N, M))
+
+    def apply_h(self, N, M, C, Ho, Hint, reps=0):
+        """(out, ms per launch averaged over `reps` timed launches, map bytes)."""
+        C = np.ascontiguousarray(C, np.complex128)
+        Hint = np.ascontiguousarray(Hint, np.complex128)
+        ho = _cuda_layout(Ho)
+        out = np.zeros(nc_of(N, M), np.complex128)
+        ms = ct.c_float(0.0)
+        err = ct.create_string_buffer(512)
+        rc = self.lib.refcuda_apply_h(N, M, _ptr(C), _ptr(ho), _ptr(Hint), _ptr(out), reps,
+                                      ct.byref(ms), err, 512)
+        if rc != 0:
+            raise RuntimeError(err.value.decode())
+        return out, float(ms.value), int(self.lib.refcuda_map_bytes())

@@ -251,3 +251,25 @@ def test_block_and_dense_pair_kernels_agree(orc, N, M, g):
     ref = orc.apply_h(N, M, C, Ho, Hint, mode=2)
     assert rel(fast, ref) <= TOL and rel(blocks, ref) <= TOL and rel(dense, ref) <= TOL
     assert rel(sp.apply_h_adjoint(C).cpu().numpy(), ref) <= TOL    # Hermitian here
+
+
+@pytest.mark.parametrize("N,M", [(2, 2), (2, 7), (3, 12), (5, 11), (7, 9), (10, 10), (6, 12), (12, 4)])
+def test_gemm_and_csr_pair_kernels_agree(orc, N, M):
+    # general (random) integrals: the dense-product kernel by default, the
+    # compressed-row kernel with MCPI_OPT_NO_GEMM_KERNEL; N=2 has one
+    # (N-2)-configuration, N=10 M=10 more tiles than the persistent grid
+    C, Ho, Hint = mc.random_problem(N, M, 71)
+    ref = orc.apply_h(N, M, C, Ho, Hint, mode=2)
+    sp = _space(N, M)
+    sp.set_integrals(Ho, Hint)
+    gemm = sp.apply_h(C).cpu().numpy()
+    adj = sp.apply_h_adjoint(C).cpu().numpy()
+    sp.set_option(4, 1)
+    sp.set_integrals(Ho, Hint)
+    csr = sp.apply_h(C).cpu().numpy()
+    assert rel(gemm, ref) <= TOL and rel(csr, ref) <= TOL and rel(adj, ref) <= TOL
+    sp.set_option(4, 0)
+    sp.set_dense_pair_kernel(True)           # the dense product also for sparse (Lieb) integrals
+    Ho2, Hint2 = mc.lieb_integrals(M, 1.5)
+    sp.set_integrals(Ho2, Hint2)
+    assert rel(sp.apply_h(C).cpu().numpy(), orc.apply_h(N, M, C, Ho2, Hint2, mode=2)) <= TOL
