@@ -41,6 +41,13 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
     asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
 }
 
+// the same, cached in L2 only (scattered 16-byte gathers with no L1 reuse)
+__device__ __forceinline__ void cp_async16_cg(void *smem, const void *gmem)
+{
+    unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+
 __device__ __forceinline__ void cp_async_wait_all()
 {
     asm volatile("cp.async.commit_group;\n"
@@ -141,99 +148,432 @@ __global__ void __launch_bounds__(kT1) k_pair_annihilate(Space sp, SpaceTables t
 }
 
 // ---------------------------------------------------------------------------
-// kernel 1, dense-product form for general pair matrices (P <= kGemmMaxP).
-// A persistent block keeps Ht (P x P, zero-padded to PA = 8 * RA rows) in
-// shared memory. Per tile of kGM (N-2)-configurations it gathers
-// D[b][m] = c_b(m) psi[index(m + pair b)] into shared memory (kTG / kGM threads
-// per configuration, cp.async), then forms E[a][m] = sum_b Ht[a][b] D[b][m] as a
-// register-tiled complex FP64 product: warp w owns the rows a = w*RA .. w*RA+RA-1
-// (Ht reads are warp-uniform broadcasts), lane owns the columns m = lane and
-// lane + 32 (conflict-free 16-byte reads of D, coalesced evict-first stores of E).
-// Per configuration: P gathers, 4 P^2 FP64 FMAs, P stores.
+// kernel 1, dense-product form for general pair matrices (P <= kGemmMaxP), on
+// the FP64 tensor cores (mma.sync m8n8k4 .f64: 8 x 8 x 4 per warp instruction).
+// A persistent block keeps Ht in shared memory. Per tile of kGM
+// (N-2)-configurations it gathers D[b][m] = c_b(m) psi[index(m + pair b)] into
+// shared memory (kTG / kGM threads per configuration, cp.async), then forms
+// E^T[m][a] = sum_b D^T[m][b] Ht^T[b][a]: MMA rows are configurations, columns
+// pairs a, the reduction runs over pairs b. Warp w owns the 8 configurations
+// m0 + 8w .. m0 + 8w + 7 and every a; per step of 4 b it loads one complex D
+// entry and NT complex Ht entries per lane (16-byte loads, conflict-free by an
+// XOR swizzle of the column index) and issues 4 NT MMAs:
+//   Er += Dr Hr + (-Di) Hi,   Ei += Dr Hi + Di Hr.
+// The accumulator layout puts 8 consecutive configurations of one a in a lane
+// quad's rows, so every E store instruction writes four full 128-byte rows.
+// Per configuration: P gathers, 4 P^2 FP64 multiply-adds, P stores.
+// Shared layout (complex entries):
+//   Hs[a][b ^ ((a & 1) << 2)]   PA x HS, zero outside a < P, b < P
+//   D[b][m ^ ((b & 3) << 1)]    PK x kGM, rows b >= P zero
 // ---------------------------------------------------------------------------
 constexpr int kTG = 256;   // threads per block, dense-product form
-constexpr int kGM = 64;    // (N-2)-configurations per tile
+constexpr int kGM = 64;    // (N-2)-configurations per tile (8 warps x 8)
+
+__device__ __forceinline__ void dmma(double &c0, double &c1, double a, double b)
+{
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+        : "+d"(c0), "+d"(c1)
+        : "d"(a), "d"(b));
+}
+
+// m16n8k4: A 16 x 4 (a0 row g, a1 row g + 8; column t), B 4 x 8 (row t, column g),
+// C 16 x 8 (c0, c1 row g, c2, c3 row g + 8; columns 2t, 2t + 1), g = lane / 4, t = lane % 4
+__device__ __forceinline__ void dmma16(double (&c)[4], double a0, double a1, double b)
+{
+    asm("mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0, %1, %2, %3}, {%4, %5}, {%6}, {%0, %1, %2, %3};\n"
+        : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+        : "d"(a0), "d"(a1), "d"(b));
+}
+
+__device__ __forceinline__ double neg(double x)
+{
+    return __hiloint2double(__double2hiint(x) ^ 0x80000000, __double2loint(x));
+}
 
 template <int M>
-__global__ void __launch_bounds__(kTG, M <= 10 ? 2 : 1) k_pair_annihilate_gemm(Space sp, SpaceTables tb,
-                                                                 const double2 *__restrict__ H,
-                                                                 const double2 *__restrict__ psi,
-                                                                 double2 *__restrict__ E, uint32_t ntiles)
+struct GemmShape {
+    static constexpr int P = M * (M + 1) / 2;
+    static constexpr int PA = (P + 7) / 8 * 8;     // a padded to whole 8-column MMA tiles
+    static constexpr int PK = (P + 3) / 4 * 4;     // b padded to whole 4-deep MMA steps
+    static constexpr int HS = (PK + 7) / 8 * 8;    // row stride of Hs (a multiple of 8 for the swizzle)
+    static constexpr int NT = PA / 8;
+    static constexpr size_t hbytes = sizeof(double2) * (size_t)PA * HS;
+    static constexpr size_t dbytes = sizeof(double2) * (size_t)PK * kGM;
+};
+
+// Gather of one tile's D (this thread's share: configuration cfg, pairs b with
+// b % kParts == part) as cp.async copies into D, committed as one group; the
+// occupations u of the configuration are returned for the scaling once the
+// copies have landed. Configurations past nc2 get zero rows.
+template <int M, int kParts>
+__device__ __forceinline__ void gemm_gather(const Space &sp, const uint32_t *W, const double2 *__restrict__ psi,
+                                            double2 *D, uint32_t m, int cfg, int part, int (&u)[M])
 {
     constexpr int P = M * (M + 1) / 2;
-    constexpr int RA = (P + 7) / 8;
-    constexpr int PA = 8 * RA;
+    if (m < sp.nc2) {
+        int Q[M];
+        decode<M>(m, sp.N - 2, sp.nc2, W, sp.wstride, u, Q);
+        uint32_t B0[M], B1[M], B2[M];
+        prefix_table<M>(Q, 0, W, sp.wstride, B0);
+        prefix_table<M>(Q, 1, W, sp.wstride, B1);
+        prefix_table<M>(Q, 2, W, sp.wstride, B2);
+#pragma unroll
+        for (int q = 0; q < M; ++q)
+#pragma unroll
+            for (int l = q; l < M; ++l) {
+                const int pb = pair_index(q, l, M);
+                if (pb % kParts == part) {
+                    const uint32_t j = idx_add2(sp.nc, B0, B1, B2, q, l, M);
+                    cp_async16_cg(D + pb * kGM + (cfg ^ ((pb & 3) << 1)), psi + j);
+                }
+            }
+    } else {
+#pragma unroll
+        for (int i = 0; i < M; ++i) u[i] = 0;
+        for (int pb = part; pb < P; pb += kParts) D[pb * kGM + (cfg ^ ((pb & 3) << 1))] = make_double2(0.0, 0.0);
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+
+// After this thread's copies have landed: D[b][m] *= c_b(m) on its share
+// (<m|a_q a_l|psi> = sqrt((u_q+1)(u_l+1)) psi_j for q < l, sqrt((u_q+1)(u_q+2)) psi_j for q = l).
+template <int M, int kParts>
+__device__ __forceinline__ void gemm_scale(const double *sq, double2 *D, const int (&u)[M], int cfg, int part)
+{
+    double r1[M], r2[M];   // sqrt(u_t + 1), sqrt((u_t + 1)(u_t + 2))
+#pragma unroll
+    for (int t = 0; t < M; ++t) {
+        r1[t] = sq[u[t] + 1];
+        r2[t] = r1[t] * sq[u[t] + 2];
+    }
+#pragma unroll
+    for (int q = 0; q < M; ++q)
+#pragma unroll
+        for (int l = q; l < M; ++l) {
+            const int pb = pair_index(q, l, M);
+            if (pb % kParts == part) {
+                const double c = (q == l) ? r2[q] : r1[q] * r1[l];
+                double2 &d = D[pb * kGM + (cfg ^ ((pb & 3) << 1))];
+                d.x *= c;
+                d.y *= c;
+            }
+        }
+}
+
+// The factors c_b(m) of this thread's configuration into Cs, from the table
+// ct (ct[x * nu + y] = sqrt(x+1) sqrt(y+1), ct[nu * nu + x] = sqrt(x+1) sqrt(x+2),
+// the products the scaling would form): shared-memory loads and stores only.
+template <int M>
+__device__ __forceinline__ void gemm_coeffs(const double *ct, int nu, double *Cs, const int (&u)[M], int cfg)
+{
+#pragma unroll
+    for (int q = 0; q < M; ++q)
+#pragma unroll
+        for (int l = q; l < M; ++l) {
+            const int pb = pair_index(q, l, M);
+            Cs[pb * kGM + (cfg ^ ((pb & 3) << 2))] = (q == l) ? ct[nu * nu + u[q]] : ct[u[q] * nu + u[l]];
+        }
+}
+
+// One tile's product on the FP64 tensor cores and the E stores (warp-level):
+// configurations m0 + 8 cg .. m0 + 8 cg + 7, pair tiles [T0, T1) (8 a each).
+template <int M, int T0, int T1>
+__device__ __forceinline__ void gemm_tile(const double2 *Hs, const double2 *D, double2 *__restrict__ E,
+                                          size_t stride, uint32_t nc2, uint32_t m0, int cg, int lane)
+{
+    using G = GemmShape<M>;
+    constexpr int P = G::P, PK = G::PK, HS = G::HS, NT = T1 - T0;
+    const int qr = lane >> 2, qc = lane & 3;      // MMA fragment row / column-in-quad
+    const int mrow = 8 * cg + qr;                 // this lane's configuration within the tile (A row)
+    double er[NT][2], ei[NT][2];
+#pragma unroll
+    for (int t = 0; t < NT; ++t) er[t][0] = er[t][1] = ei[t][0] = ei[t][1] = 0.0;
+#pragma unroll 2
+    for (int k0 = 0; k0 < PK; k0 += 4) {
+        const int b = k0 + qc;
+        const double2 d = D[b * kGM + (mrow ^ ((b & 3) << 1))];
+        const double ndi = neg(d.y);
+        double2 h[NT];
+#pragma unroll
+        for (int t = 0; t < NT; ++t) {
+            const int a = 8 * (T0 + t) + qr;
+            h[t] = Hs[a * HS + (b ^ ((a & 1) << 2))];
+        }
+        // 2 NT independent MMAs, then the 2 NT that accumulate onto them
+#pragma unroll
+        for (int t = 0; t < NT; ++t) {
+            dmma(er[t][0], er[t][1], d.x, h[t].x);
+            dmma(ei[t][0], ei[t][1], d.x, h[t].y);
+        }
+#pragma unroll
+        for (int t = 0; t < NT; ++t) {
+            dmma(er[t][0], er[t][1], ndi, h[t].y);
+            dmma(ei[t][0], ei[t][1], d.y, h[t].x);
+        }
+    }
+    const uint32_t mo = m0 + mrow;
+    if (mo < nc2) {
+#pragma unroll
+        for (int t = 0; t < NT; ++t)
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+                const int a = 8 * (T0 + t) + 2 * qc + i;
+                if (a < P) __stcs(E + a * stride + mo, make_double2(er[t][i], ei[t][i]));
+            }
+    }
+}
+
+// The same with m16n8k4 MMAs: configurations m0 + 16 mg + (0 .. 15), pair tiles [T0, T1).
+// With CS, D holds the bare gathered psi_j and Cs[b][m ^ ((b & 3) << 2)] the
+// factor c_b(m); each lane scales its two A entries before the MMAs.
+template <int M, int T0, int T1, bool CS>
+__device__ __forceinline__ void gemm_tile16(const double2 *Hs, const double2 *D, const double *Cs,
+                                            double2 *__restrict__ E, size_t stride, uint32_t nc2, uint32_t m0,
+                                            int mg, int lane)
+{
+    using G = GemmShape<M>;
+    constexpr int P = G::P, PK = G::PK, HS = G::HS, NT = T1 - T0;
+    const int qr = lane >> 2, qc = lane & 3;
+    const int mr0 = 16 * mg + qr, mr1 = mr0 + 8;  // this lane's two configurations within the tile
+    double er[NT][4], ei[NT][4];
+#pragma unroll
+    for (int t = 0; t < NT; ++t)
+#pragma unroll
+        for (int i = 0; i < 4; ++i) er[t][i] = ei[t][i] = 0.0;
+#pragma unroll 2
+    for (int k0 = 0; k0 < PK; k0 += 4) {
+        const int b = k0 + qc;
+        const int sw = (b & 3) << 1;
+        double2 d0 = D[b * kGM + (mr0 ^ sw)], d1 = D[b * kGM + (mr1 ^ sw)];
+        if constexpr (CS) {
+            const int cw = (b & 3) << 2;
+            const double c0 = Cs[b * kGM + (mr0 ^ cw)], c1 = Cs[b * kGM + (mr1 ^ cw)];
+            d0.x *= c0;
+            d0.y *= c0;
+            d1.x *= c1;
+            d1.y *= c1;
+        }
+        const double n0 = neg(d0.y), n1 = neg(d1.y);
+        double2 h[NT];
+#pragma unroll
+        for (int t = 0; t < NT; ++t) {
+            const int a = 8 * (T0 + t) + qr;
+            h[t] = Hs[a * HS + (b ^ ((a & 1) << 2))];
+        }
+#pragma unroll
+        for (int t = 0; t < NT; ++t) {
+            dmma16(er[t], d0.x, d1.x, h[t].x);
+            dmma16(ei[t], d0.x, d1.x, h[t].y);
+        }
+#pragma unroll
+        for (int t = 0; t < NT; ++t) {
+            dmma16(er[t], n0, n1, h[t].y);
+            dmma16(ei[t], d0.y, d1.y, h[t].x);
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+        const uint32_t mo = m0 + (r ? mr1 : mr0);
+        if (mo < nc2) {
+#pragma unroll
+            for (int t = 0; t < NT; ++t)
+#pragma unroll
+                for (int i = 0; i < 2; ++i) {
+                    const int a = 8 * (T0 + t) + 2 * qc + i;
+                    if (a < P) __stcs(E + a * stride + mo, make_double2(er[t][2 * r + i], ei[t][2 * r + i]));
+                }
+        }
+    }
+}
+
+template <int M>
+__device__ __forceinline__ void gemm_load_h(const double2 *__restrict__ H, double2 *Hs, int nthreads)
+{
+    using G = GemmShape<M>;
+    for (int x = threadIdx.x; x < G::PA * G::HS; x += nthreads) {
+        const int a = x / G::HS, c = x % G::HS;
+        const int b = c ^ ((a & 1) << 2);                          // logical column stored at c
+        Hs[x] = (a < G::P && b < G::P) ? H[a * G::P + b] : make_double2(0.0, 0.0);
+    }
+}
+
+// One block of 8 warps alternates gather and product on one D buffer; two
+// blocks per SM (M <= 10) overlap one's gathers with the other's MMAs. Used
+// when two D buffers do not fit shared memory.
+template <int M>
+__global__ void __launch_bounds__(kTG, M <= 10 ? 2 : 1)
+    k_pair_annihilate_gemm(Space sp, SpaceTables tb, const double2 *__restrict__ H,
+                           const double2 *__restrict__ psi, double2 *__restrict__ E, uint32_t ntiles)
+{
+    using G = GemmShape<M>;
+    constexpr int P = G::P, PA = G::PA, PK = G::PK, HS = G::HS;
     constexpr int kParts = kTG / kGM;
-    static_assert(kTG == 256 && kGM == 64, "8 warps x RA rows, 2 columns per lane");
+    static_assert(kTG == 256 && kGM == 64, "8 warps x 8 configurations");
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    double2 *Hs = reinterpret_cast<double2 *>(smem_raw);          // PA x P
-    double2 *D = Hs + PA * P;                                     // P x kGM
-    double *sq = reinterpret_cast<double *>(D + P * kGM);
+    double2 *Hs = reinterpret_cast<double2 *>(smem_raw);          // PA x HS
+    double2 *D = Hs + PA * HS;                                    // PK x kGM
+    double *sq = reinterpret_cast<double *>(D + PK * kGM);
     uint32_t *W = reinterpret_cast<uint32_t *>(sq + sp.wstride);
     load_tables(sp, tb, W, sq);
-    for (int x = threadIdx.x; x < PA * P; x += kTG) Hs[x] = x < P * P ? H[x] : make_double2(0.0, 0.0);
+    gemm_load_h<M>(H, Hs, kTG);
+    for (int x = P * kGM + threadIdx.x; x < PK * kGM; x += kTG) D[x] = make_double2(0.0, 0.0);
+    __syncthreads();
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int cfg = threadIdx.x % kGM, part = threadIdx.x / kGM;
-    const int ws = sp.wstride;
-    const size_t stride = sp.nc2;
-    const double2 *Hw = Hs + warp * RA * P;
     for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const uint32_t m0 = tile * kGM;
-        const uint32_t m = m0 + cfg;
-        __syncthreads();   // tables loaded (first tile) / previous tile's D consumed
-        if (m < sp.nc2) {
-            int u[M], Q[M];
-            decode<M>(m, sp.N - 2, sp.nc2, W, ws, u, Q);
-            uint32_t B0[M], B1[M], B2[M];
-            prefix_table<M>(Q, 0, W, ws, B0);
-            prefix_table<M>(Q, 1, W, ws, B1);
-            prefix_table<M>(Q, 2, W, ws, B2);
-#pragma unroll
-            for (int q = 0; q < M; ++q)
-#pragma unroll
-                for (int l = q; l < M; ++l)
-                    if (pair_index(q, l, M) % kParts == part) {
-                        const uint32_t j = idx_add2(sp.nc, B0, B1, B2, q, l, M);
-                        cp_async16(D + pair_index(q, l, M) * kGM + cfg, psi + j);
-                    }
-            cp_async_wait_all();
-#pragma unroll
-            for (int q = 0; q < M; ++q)
-#pragma unroll
-                for (int l = q; l < M; ++l)
-                    if (pair_index(q, l, M) % kParts == part) {
-                        const double c = (q == l) ? sq[u[q] + 1] * sq[u[q] + 2] : sq[u[q] + 1] * sq[u[l] + 1];
-                        double2 &d = D[pair_index(q, l, M) * kGM + cfg];
-                        d.x *= c;
-                        d.y *= c;
-                    }
-        } else {
-            for (int b = part; b < P; b += kParts) D[b * kGM + cfg] = make_double2(0.0, 0.0);
-        }
+        int u[M];
+        gemm_gather<M, kParts>(sp, W, psi, D, tile * kGM + cfg, cfg, part, u);
+        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+        gemm_scale<M, kParts>(sq, D, u, cfg, part);
         __syncthreads();
+        gemm_tile<M, 0, G::NT>(Hs, D, E, sp.nc2, (uint32_t)sp.nc2, tile * kGM, warp, lane);
+        __syncthreads();   // every warp done with D before the next gather
+    }
+}
 
-        double2 acc0[RA], acc1[RA];
+// Warp-specialised form (one block per SM): warps 0-15 run the products with
+// m16n8k4 MMAs (warp w takes configurations 16 (w & 3) .. 16 (w & 3) + 15 of
+// the tile and quarter w >> 2 of the pair tiles, so each SM sub-partition runs
+// all pair tiles of one group of 16 configurations), warps 16-19 gather the next
+// tiles into the other NS - 1 D buffers meanwhile: one thread per configuration
+// (decoded once, all P gathers and scalings), warps 16-17 for the even tiles of
+// the block, 18-19 for the odd ones. Tile i of a block uses buffer i % NS.
+// Hand-over by mbarriers:
+//   full[b]  : the 64 gather threads of the tile arrive after scaling buffer b; product
+//              warps wait on its phase (tile i: parity (i / NS) & 1);
+//   empty[b] : lane 0 of each of the 16 product warps arrives after reading
+//              buffer b when a later tile of this block reuses it (i + NS < its
+//              tile count); the gatherers wait on it (tile i >= NS: parity
+//              (i / NS - 1) & 1) before overwriting.
+// Product warps never wait for one another. Every wait is bounded: after
+// kWaitCycles the thread records the timeout in the status word and returns
+// (with no copies of its own in flight), so a stuck pipeline ends the kernel
+// with an error instead of hanging.
+constexpr int kTW = 2 * kTG + 2 * kGM;   // threads per block, warp-specialised form
+constexpr long long kWaitCycles = 4000000000LL;
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_addr(bar)) : "memory");
+}
+
+// true once the phase of the given parity has completed; false after kWaitCycles
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
+{
+    const long long t0 = clock64();
+    for (;;) {
+        uint32_t ok;
+        asm volatile(
+            "{\n"
+            ".reg .pred p;\n"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+            "selp.u32 %0, 1, 0, p;\n"
+            "}\n"
+            : "=r"(ok)
+            : "r"(smem_addr(bar)), "r"(parity)
+            : "memory");
+        if (ok) return true;
+        if (clock64() - t0 > kWaitCycles) return false;
+    }
+}
+
+template <int M, int NS, bool CS>
+__global__ void __launch_bounds__(kTW, 1)
+    k_pair_annihilate_gemm_ws(Space sp, SpaceTables tb, const double2 *__restrict__ H,
+                              const double2 *__restrict__ psi, double2 *__restrict__ E, uint32_t ntiles,
+                              int *status)
+{
+    using G = GemmShape<M>;
+    constexpr int P = G::P, PA = G::PA, PK = G::PK, HS = G::HS;
+    constexpr int kProdThreads = 2 * kTG;
+    constexpr int kGroups = (kTW - kProdThreads) / kGM;   // gather groups of kGM threads
+    static_assert(kTG == 256 && kGM == 64 && kGroups == 2, "16 product warps, 2 x 2 gather warps");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2 *Hs = reinterpret_cast<double2 *>(smem_raw);          // PA x HS
+    double2 *Dbuf = Hs + PA * HS;                                 // NS x (PK x kGM)
+    double *Cbuf = reinterpret_cast<double *>(Dbuf + NS * PK * kGM);      // NS x (PK x kGM) when CS
+    uint64_t *full = reinterpret_cast<uint64_t *>(Cbuf + (CS ? NS * PK * kGM : 0));  // NS
+    uint64_t *empty = full + NS;                                           // NS
+    double *sq = reinterpret_cast<double *>(empty + NS);
+    const int nu = sp.N - 1;                                       // occupations 0 .. N-2
+    double *ct = sq + sp.wstride;                                  // nu * nu + nu when CS
+    uint32_t *W = reinterpret_cast<uint32_t *>(ct + (CS ? nu * nu + nu : 0));
+    load_tables(sp, tb, W, sq);
+    gemm_load_h<M>(H, Hs, kTW);
+    for (int x = P * kGM + threadIdx.x; x < PK * kGM; x += kTW)
 #pragma unroll
-        for (int i = 0; i < RA; ++i) acc0[i] = acc1[i] = make_double2(0.0, 0.0);
-#pragma unroll 5
-        for (int k = 0; k < P; ++k) {
-            const double2 d0 = D[k * kGM + lane], d1 = D[k * kGM + lane + 32];
-#pragma unroll
-            for (int i = 0; i < RA; ++i) {
-                const double2 h = Hw[i * P + k];
-                cfma(acc0[i], h, d0);
-                cfma(acc1[i], h, d1);
-            }
+        for (int b = 0; b < NS; ++b) {
+            Dbuf[b * PK * kGM + x] = make_double2(0.0, 0.0);
+            if (CS) Cbuf[b * PK * kGM + x] = 0.0;
         }
-        const bool ok0 = m0 + lane < sp.nc2, ok1 = m0 + lane + 32 < sp.nc2;
+    if (CS) {
+        __syncthreads();   // sq loaded
+        for (int x = threadIdx.x; x < nu * nu + nu; x += kTW)
+            ct[x] = x < nu * nu ? sq[x / nu + 1] * sq[x % nu + 1] : sq[x - nu * nu + 1] * sq[x - nu * nu + 2];
+    }
+    if (threadIdx.x == 0)
 #pragma unroll
-        for (int i = 0; i < RA; ++i) {
-            const int a = warp * RA + i;
-            if (a < P) {
-                if (ok0) __stcs(E + a * stride + m0 + lane, acc0[i]);
-                if (ok1) __stcs(E + a * stride + m0 + lane + 32, acc1[i]);
+        for (int b = 0; b < NS; ++b) {
+            mbar_init(full + b, kGM);
+            mbar_init(empty + b, kProdThreads / 32);
+        }
+    __syncthreads();
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t ntb = blockIdx.x < ntiles ? (ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+    if (warp >= kProdThreads / 32) {
+        const int g = threadIdx.x - kProdThreads;
+        const int cfg = g % kGM, grp = g / kGM;
+        for (uint32_t i = grp; i < ntb; i += kGroups) {
+            const int buf = i % NS;
+            double2 *D = Dbuf + buf * PK * kGM;
+            if (i >= NS && !mbar_wait(empty + buf, (i / NS - 1) & 1)) {
+                atomicExch(status, 1);
+                return;
             }
+            int u[M];
+            gemm_gather<M, 1>(sp, W, psi, D, (blockIdx.x + i * gridDim.x) * kGM + cfg, cfg, 0, u);
+            if constexpr (CS) gemm_coeffs<M>(ct, nu, Cbuf + buf * PK * kGM, u, cfg);
+            asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+            if constexpr (!CS) gemm_scale<M, 1>(sq, D, u, cfg, 0);
+            mbar_arrive(full + buf);
+        }
+    } else {
+        constexpr int NT = G::NT;
+        constexpr int T1 = (NT + 3) / 4, T2 = (2 * NT + 3) / 4, T3 = (3 * NT + 3) / 4;
+        const int mg = warp & 3, ap = warp >> 2;
+        for (uint32_t i = 0; i < ntb; ++i) {
+            const int buf = i % NS;
+            if (!mbar_wait(full + buf, (i / NS) & 1)) {
+                if (lane == 0) atomicExch(status, 1);
+                return;
+            }
+            const uint32_t m0 = (blockIdx.x + i * gridDim.x) * kGM;
+            const double2 *D = Dbuf + buf * PK * kGM;
+            const double *Cs = Cbuf + buf * PK * kGM;
+            const uint32_t n2 = (uint32_t)sp.nc2;
+            if (ap == 0) {
+                gemm_tile16<M, 0, T1, CS>(Hs, D, Cs, E, sp.nc2, n2, m0, mg, lane);
+            } else if (ap == 1) {
+                if constexpr (T1 < T2) gemm_tile16<M, T1, T2, CS>(Hs, D, Cs, E, sp.nc2, n2, m0, mg, lane);
+            } else if (ap == 2) {
+                if constexpr (T2 < T3) gemm_tile16<M, T2, T3, CS>(Hs, D, Cs, E, sp.nc2, n2, m0, mg, lane);
+            } else {
+                if constexpr (T3 < NT) gemm_tile16<M, T3, NT, CS>(Hs, D, Cs, E, sp.nc2, n2, m0, mg, lane);
+            }
+            __syncwarp();
+            if (lane == 0 && i + NS < ntb) mbar_arrive(empty + buf);
         }
     }
 }
@@ -637,17 +977,51 @@ cudaError_t apply_h_m(const Space &sp, const SpaceTables &tb, const PairOp &op, 
         k_pair_annihilate_blocks<M><<<g1, kT1b, smb, st>>>(sp, tb, bo, psi, E);
     } else if (sp.N >= 2 && (stages & 1) && op.hdense && P <= kGemmMaxP) {
         if constexpr (P <= kGemmMaxP) {
-            constexpr int PA = 8 * ((P + 7) / 8);
-            const size_t smg = sizeof(double2) * (PA * P + P * kGM) + tab;
-            cudaError_t e = cudaFuncSetAttribute(k_pair_annihilate_gemm<M>,
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smg);
-            if (e != cudaSuccess) return e;
-            int dev = 0, sms = 0;
+            using G = GemmShape<M>;
+            int dev = 0, sms = 0, optin = 0;
+            cudaError_t e;
             if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
             if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+            if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev)) != cudaSuccess)
+                return e;
             const uint32_t ntiles = (uint32_t)((sp.nc2 + kGM - 1) / kGM);
-            const unsigned g1 = ntiles < 2u * sms ? ntiles : 2u * sms;
-            if (g1) k_pair_annihilate_gemm<M><<<g1, kTG, smg, st>>>(sp, tb, op.hdense, psi, E, ntiles);
+            const size_t nu = (size_t)sp.N - 1;
+            const size_t cbytes = G::dbytes / 2;   // PK x kGM doubles
+            const size_t smc2 = G::hbytes + 2 * (G::dbytes + cbytes) + 4 * sizeof(uint64_t) +
+                                sizeof(double) * (nu * nu + nu) + tab;
+            const size_t smw3 = G::hbytes + 3 * G::dbytes + 6 * sizeof(uint64_t) + tab;
+            const size_t smw2 = G::hbytes + 2 * G::dbytes + 4 * sizeof(uint64_t) + tab;
+            const unsigned gw = ntiles < (uint32_t)sms ? ntiles : (uint32_t)sms;
+            if (smc2 <= (size_t)optin) {
+                if ((e = cudaFuncSetAttribute(k_pair_annihilate_gemm_ws<M, 2, true>,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smc2)) != cudaSuccess)
+                    return e;
+                if (gw)
+                    k_pair_annihilate_gemm_ws<M, 2, true>
+                        <<<gw, kTW, smc2, st>>>(sp, tb, op.hdense, psi, E, ntiles, op.status);
+            } else if (smw3 <= (size_t)optin) {
+                if ((e = cudaFuncSetAttribute(k_pair_annihilate_gemm_ws<M, 3, false>,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smw3)) != cudaSuccess)
+                    return e;
+                if (gw)
+                    k_pair_annihilate_gemm_ws<M, 3, false>
+                        <<<gw, kTW, smw3, st>>>(sp, tb, op.hdense, psi, E, ntiles, op.status);
+            } else if (smw2 <= (size_t)optin) {
+                if ((e = cudaFuncSetAttribute(k_pair_annihilate_gemm_ws<M, 2, false>,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smw2)) != cudaSuccess)
+                    return e;
+                if (gw)
+                    k_pair_annihilate_gemm_ws<M, 2, false>
+                        <<<gw, kTW, smw2, st>>>(sp, tb, op.hdense, psi, E, ntiles, op.status);
+            } else {
+                const size_t smg = G::hbytes + G::dbytes + tab;
+                if ((e = cudaFuncSetAttribute(k_pair_annihilate_gemm<M>,
+                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smg)) != cudaSuccess)
+                    return e;
+                const uint32_t per_sm = M <= 10 ? 2u : 1u;
+                const unsigned g1 = ntiles < per_sm * sms ? ntiles : per_sm * sms;
+                if (g1) k_pair_annihilate_gemm<M><<<g1, kTG, smg, st>>>(sp, tb, op.hdense, psi, E, ntiles);
+            }
         }
     } else if (sp.N >= 2 && (stages & 1)) {
         const int st_nnz = op.nnz <= kCsrStaged ? op.nnz : 0;
