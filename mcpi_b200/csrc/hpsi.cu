@@ -149,32 +149,29 @@ __global__ void __launch_bounds__(kT1) k_pair_annihilate(Space sp, SpaceTables t
 
 // ---------------------------------------------------------------------------
 // kernel 1, dense-product form for general pair matrices (P <= kGemmMaxP), on
-// the FP64 tensor cores (mma.sync m8n8k4 .f64: 8 x 8 x 4 per warp instruction).
+// the FP64 tensor cores (mma.sync m16n8k4 .f64: 16 x 8 x 4 per warp instruction).
 // A persistent block keeps Ht in shared memory. Per tile of kGM
 // (N-2)-configurations it gathers D[b][m] = c_b(m) psi[index(m + pair b)] into
-// shared memory (kTG / kGM threads per configuration, cp.async), then forms
-// E^T[m][a] = sum_b D^T[m][b] Ht^T[b][a]: MMA rows are configurations, columns
-// pairs a, the reduction runs over pairs b. Warp w owns the 8 configurations
-// m0 + 8w .. m0 + 8w + 7 and every a; per step of 4 b it loads one complex D
-// entry and NT complex Ht entries per lane (16-byte loads, conflict-free by an
-// XOR swizzle of the column index) and issues 4 NT MMAs:
-//   Er += Dr Hr + (-Di) Hi,   Ei += Dr Hi + Di Hr.
-// The accumulator layout puts 8 consecutive configurations of one a in a lane
-// quad's rows, so every E store instruction writes four full 128-byte rows.
-// Per configuration: P gathers, 4 P^2 FP64 multiply-adds, P stores.
-// Shared layout (complex entries):
+// shared memory (cp.async), then forms E^T[m][a] = sum_b D^T[m][b] Ht^T[b][a]:
+// MMA rows are configurations, columns pairs a, the reduction runs over pairs b.
+// A warp owns 16 configurations and a range of 8-pair column tiles; per step of
+// 4 b it loads two complex D entries and one complex Ht entry per column tile
+// per lane (16-byte loads, conflict-free by XOR swizzles of the column index)
+// and forms the complex product from three real ones,
+//   t1 += Dr Hr,  t2 += Di Hi,  t3 += (Dr + Di)(Hr + Hi);  Er = t1 - t2, Ei = t3 - t1 - t2,
+// which saves a quarter of the MMAs. The accumulator layout puts 8 consecutive
+// configurations of one a in a lane quad's rows, so each E store instruction
+// writes four full 128-byte rows.
+// Per configuration: P gathers, 3 P^2 FP64 multiply-adds on the tensor cores
+// (4 P^2 algorithmic), P stores.
+// Shared layout (complex entries unless noted):
 //   Hs[a][b ^ ((a & 1) << 2)]   PA x HS, zero outside a < P, b < P
 //   D[b][m ^ ((b & 3) << 1)]    PK x kGM, rows b >= P zero
+//   Cs[b][m ^ ((b & 3) << 2)]   PK x kGM doubles (warp-specialised form with
+//                               the scaling in the product warps), rows b >= P zero
 // ---------------------------------------------------------------------------
 constexpr int kTG = 256;   // threads per block, dense-product form
 constexpr int kGM = 64;    // (N-2)-configurations per tile (8 warps x 8)
-
-__device__ __forceinline__ void dmma(double &c0, double &c1, double a, double b)
-{
-    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
-        : "+d"(c0), "+d"(c1)
-        : "d"(a), "d"(b));
-}
 
 // m16n8k4: A 16 x 4 (a0 row g, a1 row g + 8; column t), B 4 x 8 (row t, column g),
 // C 16 x 8 (c0, c1 row g, c2, c3 row g + 8; columns 2t, 2t + 1), g = lane / 4, t = lane % 4
@@ -183,11 +180,6 @@ __device__ __forceinline__ void dmma16(double (&c)[4], double a0, double a1, dou
     asm("mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0, %1, %2, %3}, {%4, %5}, {%6}, {%0, %1, %2, %3};\n"
         : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
         : "d"(a0), "d"(a1), "d"(b));
-}
-
-__device__ __forceinline__ double neg(double x)
-{
-    return __hiloint2double(__double2hiint(x) ^ 0x80000000, __double2loint(x));
 }
 
 template <int M>
@@ -275,55 +267,8 @@ __device__ __forceinline__ void gemm_coeffs(const double *ct, int nu, double *Cs
         }
 }
 
-// One tile's product on the FP64 tensor cores and the E stores (warp-level):
-// configurations m0 + 8 cg .. m0 + 8 cg + 7, pair tiles [T0, T1) (8 a each).
-template <int M, int T0, int T1>
-__device__ __forceinline__ void gemm_tile(const double2 *Hs, const double2 *D, double2 *__restrict__ E,
-                                          size_t stride, uint32_t nc2, uint32_t m0, int cg, int lane)
-{
-    using G = GemmShape<M>;
-    constexpr int P = G::P, PK = G::PK, HS = G::HS, NT = T1 - T0;
-    const int qr = lane >> 2, qc = lane & 3;      // MMA fragment row / column-in-quad
-    const int mrow = 8 * cg + qr;                 // this lane's configuration within the tile (A row)
-    double er[NT][2], ei[NT][2];
-#pragma unroll
-    for (int t = 0; t < NT; ++t) er[t][0] = er[t][1] = ei[t][0] = ei[t][1] = 0.0;
-#pragma unroll 2
-    for (int k0 = 0; k0 < PK; k0 += 4) {
-        const int b = k0 + qc;
-        const double2 d = D[b * kGM + (mrow ^ ((b & 3) << 1))];
-        const double ndi = neg(d.y);
-        double2 h[NT];
-#pragma unroll
-        for (int t = 0; t < NT; ++t) {
-            const int a = 8 * (T0 + t) + qr;
-            h[t] = Hs[a * HS + (b ^ ((a & 1) << 2))];
-        }
-        // 2 NT independent MMAs, then the 2 NT that accumulate onto them
-#pragma unroll
-        for (int t = 0; t < NT; ++t) {
-            dmma(er[t][0], er[t][1], d.x, h[t].x);
-            dmma(ei[t][0], ei[t][1], d.x, h[t].y);
-        }
-#pragma unroll
-        for (int t = 0; t < NT; ++t) {
-            dmma(er[t][0], er[t][1], ndi, h[t].y);
-            dmma(ei[t][0], ei[t][1], d.y, h[t].x);
-        }
-    }
-    const uint32_t mo = m0 + mrow;
-    if (mo < nc2) {
-#pragma unroll
-        for (int t = 0; t < NT; ++t)
-#pragma unroll
-            for (int i = 0; i < 2; ++i) {
-                const int a = 8 * (T0 + t) + 2 * qc + i;
-                if (a < P) __stcs(E + a * stride + mo, make_double2(er[t][i], ei[t][i]));
-            }
-    }
-}
-
-// The same with m16n8k4 MMAs: configurations m0 + 16 mg + (0 .. 15), pair tiles [T0, T1).
+// One tile's product on the FP64 tensor cores (m16n8k4) and the E stores
+// (warp-level): configurations m0 + 16 mg + (0 .. 15), pair tiles [T0, T1) (8 a each).
 // With CS, D holds the bare gathered psi_j and Cs[b][m ^ ((b & 3) << 2)] the
 // factor c_b(m); each lane scales its two A entries before the MMAs.
 template <int M, int T0, int T1, bool CS>
@@ -335,11 +280,13 @@ __device__ __forceinline__ void gemm_tile16(const double2 *Hs, const double2 *D,
     constexpr int P = G::P, PK = G::PK, HS = G::HS, NT = T1 - T0;
     const int qr = lane >> 2, qc = lane & 3;
     const int mr0 = 16 * mg + qr, mr1 = mr0 + 8;  // this lane's two configurations within the tile
-    double er[NT][4], ei[NT][4];
+    // complex product in three real products: t1 = Dr Hr, t2 = Di Hi,
+    // t3 = (Dr + Di)(Hr + Hi); Er = t1 - t2, Ei = t3 - t1 - t2
+    double t1[NT][4], t2[NT][4], t3[NT][4];
 #pragma unroll
     for (int t = 0; t < NT; ++t)
 #pragma unroll
-        for (int i = 0; i < 4; ++i) er[t][i] = ei[t][i] = 0.0;
+        for (int i = 0; i < 4; ++i) t1[t][i] = t2[t][i] = t3[t][i] = 0.0;
 #pragma unroll 2
     for (int k0 = 0; k0 < PK; k0 += 4) {
         const int b = k0 + qc;
@@ -353,7 +300,7 @@ __device__ __forceinline__ void gemm_tile16(const double2 *Hs, const double2 *D,
             d1.x *= c1;
             d1.y *= c1;
         }
-        const double n0 = neg(d0.y), n1 = neg(d1.y);
+        const double s0 = d0.x + d0.y, s1 = d1.x + d1.y;
         double2 h[NT];
 #pragma unroll
         for (int t = 0; t < NT; ++t) {
@@ -362,13 +309,9 @@ __device__ __forceinline__ void gemm_tile16(const double2 *Hs, const double2 *D,
         }
 #pragma unroll
         for (int t = 0; t < NT; ++t) {
-            dmma16(er[t], d0.x, d1.x, h[t].x);
-            dmma16(ei[t], d0.x, d1.x, h[t].y);
-        }
-#pragma unroll
-        for (int t = 0; t < NT; ++t) {
-            dmma16(er[t], n0, n1, h[t].y);
-            dmma16(ei[t], d0.y, d1.y, h[t].x);
+            dmma16(t1[t], d0.x, d1.x, h[t].x);
+            dmma16(t2[t], d0.y, d1.y, h[t].y);
+            dmma16(t3[t], s0, s1, h[t].x + h[t].y);
         }
     }
 #pragma unroll
@@ -380,7 +323,9 @@ __device__ __forceinline__ void gemm_tile16(const double2 *Hs, const double2 *D,
 #pragma unroll
                 for (int i = 0; i < 2; ++i) {
                     const int a = 8 * (T0 + t) + 2 * qc + i;
-                    if (a < P) __stcs(E + a * stride + mo, make_double2(er[t][2 * r + i], ei[t][2 * r + i]));
+                    const int c = 2 * r + i;
+                    if (a < P)
+                        __stcs(E + a * stride + mo, make_double2(t1[t][c] - t2[t][c], t3[t][c] - t1[t][c] - t2[t][c]));
                 }
         }
     }
@@ -397,9 +342,10 @@ __device__ __forceinline__ void gemm_load_h(const double2 *__restrict__ H, doubl
     }
 }
 
-// One block of 8 warps alternates gather and product on one D buffer; two
-// blocks per SM (M <= 10) overlap one's gathers with the other's MMAs. Used
-// when two D buffers do not fit shared memory.
+// One block of 8 warps alternates gather and product on one D buffer (warp w:
+// configurations 16 (w & 3) .. + 15, first or second half of the pair tiles);
+// two blocks per SM (M <= 10) overlap one's gathers with the other's MMAs.
+// Used when two D buffers do not fit shared memory.
 template <int M>
 __global__ void __launch_bounds__(kTG, M <= 10 ? 2 : 1)
     k_pair_annihilate_gemm(Space sp, SpaceTables tb, const double2 *__restrict__ H,
@@ -427,7 +373,12 @@ __global__ void __launch_bounds__(kTG, M <= 10 ? 2 : 1)
         asm volatile("cp.async.wait_group 0;\n" ::: "memory");
         gemm_scale<M, kParts>(sq, D, u, cfg, part);
         __syncthreads();
-        gemm_tile<M, 0, G::NT>(Hs, D, E, sp.nc2, (uint32_t)sp.nc2, tile * kGM, warp, lane);
+        constexpr int NH = (G::NT + 1) / 2;
+        const int mg = warp & 3;
+        if (warp < 4)
+            gemm_tile16<M, 0, NH, false>(Hs, D, nullptr, E, sp.nc2, (uint32_t)sp.nc2, tile * kGM, mg, lane);
+        else if constexpr (NH < G::NT)
+            gemm_tile16<M, NH, G::NT, false>(Hs, D, nullptr, E, sp.nc2, (uint32_t)sp.nc2, tile * kGM, mg, lane);
         __syncthreads();   // every warp done with D before the next gather
     }
 }
