@@ -11,7 +11,8 @@ the states resident in HBM, eight distinct states rotating between steps
 `e2e` is the same metric through the public API with the state copied from
 pinned host memory and the result copied back inside every step. The line
 also carries the roofline of the dominant kernel (CUDA events, measured live),
-a 150-step Lanczos ground-state solve of the same configuration, and the CPU
+a 150-step Lanczos ground-state solve of the same configuration, H.psi with
+general (dense pair matrix) integrals at N=10 and N=16, M=10, and the CPU
 baseline: the oracle's restatement of the reference's applyHconf_X
 (hamiltonianMatrix.h:431-887; the reference's fastest CPU H.psi that runs at
 this size) on a bounded row sample with all host threads.
@@ -55,6 +56,7 @@ def parse():
     p.add_argument("--no-lanczos", action="store_true")
     p.add_argument("--no-batch", action="store_true")
     p.add_argument("--no-large", action="store_true")
+    p.add_argument("--no-general", action="store_true")
     return p.parse_args()
 
 
@@ -244,6 +246,66 @@ def run_large(mc, torch, device):
             "lanczos_iterations": it, "E0": E0, "lanczos_seconds": t_lz,
             "rho1_ms": 1e3 * t_r1, "rho2_ms": 1e3 * t_r2,
             "occupations": [round(float(o), 6) for o in occ]}
+
+
+def fp64_gemm_peak(torch, device):
+    """Measured FP64 reference: cuBLAS DGEMM 8192^3, best of 5 (TFLOP/s)."""
+    a = torch.randn(8192, 8192, dtype=torch.float64, device=device)
+    b = torch.randn_like(a)
+    for _ in range(2):
+        c = a @ b
+    best = float("inf")
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        c = a @ b
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b, c
+    torch.cuda.empty_cache()
+    return 2 * 8192 ** 3 / (best * 1e-3) / 1e12
+
+
+def run_general(mc, torch, device):
+    """General (non-momentum-conserving) integrals: random Hermitian Ho and an
+    8-fold-symmetrised random Hint, so the pair matrix is dense and kernel 1
+    runs as the FP64 tensor-core product. N=10, M=10 (nc = 92,378) and N=16,
+    M=10 (nc = 2,042,975); kernel 1 against the measured cuBLAS DGEMM rate
+    (algorithmic 8 P^2 nc2 FLOP per launch)."""
+    peak = fp64_gemm_peak(torch, device)
+    out = {"fp64_peak_tflops": peak, "fp64_peak_source": "cuBLAS DGEMM 8192^3 measured in this run"}
+    for (N, M) in [(10, 10), (16, 10)]:
+        sp = mc.FockSpace(N, M, device=device)
+        _, Ho, Hint = mc.random_problem(4, M, 91)
+        sp.set_integrals(Ho, Hint)
+        nc2, P = mc.nc_of(N - 2, M), sp.P
+        gen = torch.Generator(device=sp.torch_device)
+        gen.manual_seed(500 + N)
+        X = torch.randn((ROTATE, sp.nc), dtype=torch.complex128, device=sp.torch_device, generator=gen)
+        y = torch.empty(sp.nc, dtype=torch.complex128, device=sp.torch_device)
+        for w in range(5):
+            sp.apply_h(X[w % ROTATE], y)
+        torch.cuda.synchronize()
+        reps = 50
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for k in range(reps):
+            sp.apply_h(X[k % ROTATE], y)
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / reps
+        k1, k2 = sp.apply_h_profile(X[0], y, reps=20)
+        flops = 8.0 * P * P * nc2
+        tf = flops / (k1 * 1e-3) / 1e12
+        out[f"n{N}_m{M}"] = {"workload": f"random integrals N={N} M={M} (nc={sp.nc})", "hpsi_ms": ms,
+                             "hpsi_per_s": 1e3 / ms, "pair_annihilate_ms": k1, "pair_create_ms": k2,
+                             "pair_annihilate_tflops": tf, "pair_annihilate_frac_of_dgemm": tf / peak,
+                             "pair_annihilate_flops": flops}
+        sp.close()
+        del X, y
+        torch.cuda.empty_cache()
+    return out
 
 
 def cpu_setup(N, M, g):
@@ -452,6 +514,9 @@ def run_mcpi(args):
     large = None
     if not args.no_large:
         large = run_large(mc, torch, local)
+    general = None
+    if not args.no_general:
+        general = run_general(mc, torch, local)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -463,7 +528,7 @@ def run_mcpi(args):
                 "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
                 "config": config(), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": 2 * args.steps, "clocks": clk, "lanczos": lanczos, "batched": batched,
-                "large": large}
+                "large": large, "general": general}
         print(json.dumps(line), flush=True)
     sp.close()
     if world > 1:
