@@ -112,6 +112,15 @@ MCPI_API int mcpi_set_integrals(mcpi_space sp, const double *h_Ho, const double 
 /* out = H C (hamiltonianMatrix.h:891-1425 applyHconf_XX semantics; _omp, _X and
  * the CUDA applyHconf kernel compute the same; MCPI_VARIANT_HASH gives applyHconf). */
 MCPI_API int mcpi_apply_h(mcpi_space sp, const void *d_C, void *d_out);
+/* out_k = H C_k for k = 0 .. count-1 with C_k and out_k in HOST memory (nc
+ * complex doubles each; page-locked memory from cudaHostAlloc or
+ * cudaHostRegister gets full PCIe bandwidth). The states stream through two
+ * device buffer pairs held by the space: the copy in of state k+1, H.psi of
+ * state k and the copy out of state k-1 run concurrently on three streams.
+ * Returns when every out_k is written. The same result as count calls of the
+ * reference's applyHconf* on host arrays (hamiltonianMatrix.h:891-1425), which
+ * copy and compute one state at a time. */
+MCPI_API int mcpi_apply_h_host(mcpi_space sp, int count, const void *const *h_C, void *const *h_out);
 /* Rows [row0, row1) of H C into d_out[0 .. row1-row0), d_C being the whole
  * vector: the local part of a row-sharded H.psi (each rank owns a row block
  * and gathers the full vector first). Needs N >= 2. No reference counterpart. */

@@ -76,6 +76,7 @@ def lib():
         "mcpi_apply_h": (i, [_vp, _vp, _vp]),
         "mcpi_apply_h_adjoint": (i, [_vp, _vp, _vp]),
         "mcpi_apply_h_rows": (i, [_vp, _vp, i64, i64, _vp]),
+        "mcpi_apply_h_host": (i, [_vp, i, _vp, _vp]),
         "mcpi_apply_h_profile": (i, [_vp, _vp, _vp, i, _vp]),
         "mcpi_rho1": (i, [_vp, _vp, _vp]),
         "mcpi_rho2": (i, [_vp, _vp, _vp]),
@@ -285,6 +286,31 @@ class FockSpace:
         self._stream()
         _check(lib().mcpi_apply_h(self._h, _vp(C.data_ptr()), _vp(out.data_ptr())))
         return out
+
+    def apply_h_host(self, states, outs):
+        """outs[k] = H states[k] for host arrays (numpy complex128 or CPU torch
+        tensors, nc entries, contiguous; page-locked memory copies fastest),
+        pipelined through the device by mcpi_apply_h_host."""
+        torch = _torch()
+        if len(states) != len(outs):
+            raise MCPIError(1, "states and outs differ in length")
+
+        def ptr(x, writable):
+            if isinstance(x, np.ndarray):
+                if x.dtype != np.complex128 or not x.flags.c_contiguous or x.size != self.nc or \
+                        (writable and not x.flags.writeable):
+                    raise MCPIError(1, f"expected a contiguous complex128 array of {self.nc} entries")
+                return x.ctypes.data
+            if x.dtype != torch.complex128 or x.device.type != "cpu" or not x.is_contiguous() or x.numel() != self.nc:
+                raise MCPIError(1, f"expected a contiguous CPU complex128 tensor of {self.nc} entries")
+            return x.data_ptr()
+
+        n = len(states)
+        pin = (ct.c_void_p * max(n, 1))(*[ptr(x, False) for x in states])
+        pout = (ct.c_void_p * max(n, 1))(*[ptr(x, True) for x in outs])
+        self._stream()
+        _check(lib().mcpi_apply_h_host(self._h, n, ct.cast(pin, ct.c_void_p), ct.cast(pout, ct.c_void_p)))
+        return outs
 
     def apply_h_rows(self, C, row0: int, row1: int, out=None):
         """Rows [row0, row1) of H C (C the whole vector)."""

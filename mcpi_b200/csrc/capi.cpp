@@ -446,6 +446,17 @@ int mcpi_space_destroy(mcpi_space sp)
     cudaFree(sp->d_gram);
     cudaFree(sp->d_dot);
     cudaFree(sp->d_status);
+    if (sp->s_h2d) cudaStreamSynchronize(sp->s_h2d);
+    if (sp->s_d2h) cudaStreamSynchronize(sp->s_d2h);
+    for (int b = 0; b < 2; ++b) {
+        cudaFree(sp->d_hin[b]);
+        cudaFree(sp->d_hout[b]);
+        if (sp->ev_in[b]) cudaEventDestroy(sp->ev_in[b]);
+        if (sp->ev_comp[b]) cudaEventDestroy(sp->ev_comp[b]);
+        if (sp->ev_out[b]) cudaEventDestroy(sp->ev_out[b]);
+    }
+    if (sp->s_h2d) cudaStreamDestroy(sp->s_h2d);
+    if (sp->s_d2h) cudaStreamDestroy(sp->s_d2h);
     if (sp->own) cudaStreamDestroy(sp->own);
     delete sp;
     return MCPI_OK;
@@ -684,6 +695,47 @@ int mcpi_set_integrals(mcpi_space sp, const double *h_Ho, const double *h_Hint, 
 }
 
 int mcpi_apply_h(mcpi_space sp, const void *d_C, void *d_out) { return apply_op(sp, sp ? sp->fwd : DevPairOp{}, d_C, d_out); }
+
+int mcpi_apply_h_host(mcpi_space sp, int count, const void *const *h_C, void *const *h_out)
+{
+    CHECK_ARG(sp && count >= 0 && (count == 0 || (h_C && h_out)), "mcpi_apply_h_host: bad arguments");
+    if (!sp->has_op) return fail(MCPI_ERR_STATE, "mcpi_set_integrals has not been called");
+    for (int k = 0; k < count; ++k) CHECK_ARG(h_C[k] && h_out[k], "mcpi_apply_h_host: null state pointer");
+    DeviceGuard g(sp->device);
+    int rc = ensure_E(sp);
+    if (rc) return rc;
+    const size_t bytes = sizeof(double2) * (size_t)sp->nc;
+    if (!sp->s_h2d) {
+        CK(cudaStreamCreateWithFlags(&sp->s_h2d, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithFlags(&sp->s_d2h, cudaStreamNonBlocking));
+        for (int b = 0; b < 2; ++b) {
+            CK(cudaMalloc(&sp->d_hin[b], bytes));
+            CK(cudaMalloc(&sp->d_hout[b], bytes));
+            CK(cudaEventCreateWithFlags(&sp->ev_in[b], cudaEventDisableTiming));
+            CK(cudaEventCreateWithFlags(&sp->ev_comp[b], cudaEventDisableTiming));
+            CK(cudaEventCreateWithFlags(&sp->ev_out[b], cudaEventDisableTiming));
+        }
+    }
+    // buffer pair b = k & 1: its input is free once H.psi of state k-2 has run,
+    // its output once the copy out of state k-2 has finished
+    for (int k = 0; k < count; ++k) {
+        const int b = k & 1;
+        if (k >= 2) CK(cudaStreamWaitEvent(sp->s_h2d, sp->ev_comp[b], 0));
+        CK(cudaMemcpyAsync(sp->d_hin[b], h_C[k], bytes, cudaMemcpyHostToDevice, sp->s_h2d));
+        CK(cudaEventRecord(sp->ev_in[b], sp->s_h2d));
+        CK(cudaStreamWaitEvent(sp->stream, sp->ev_in[b], 0));
+        if (k >= 2) CK(cudaStreamWaitEvent(sp->stream, sp->ev_out[b], 0));
+        CK(mcpi::launch_apply_h(sp->sp, sp->tables(), sp->fwd.view(), sp->fwd.blocks(), sp->d_hin[b], sp->d_E,
+                                sp->d_hout[b], sp->stream));
+        CK(cudaEventRecord(sp->ev_comp[b], sp->stream));
+        CK(cudaStreamWaitEvent(sp->s_d2h, sp->ev_comp[b], 0));
+        CK(cudaMemcpyAsync(h_out[k], sp->d_hout[b], bytes, cudaMemcpyDeviceToHost, sp->s_d2h));
+        CK(cudaEventRecord(sp->ev_out[b], sp->s_d2h));
+    }
+    CK(cudaStreamSynchronize(sp->s_d2h));
+    CK(cudaStreamSynchronize(sp->stream));
+    return check_status(sp);
+}
 
 int mcpi_apply_h_profile(mcpi_space sp, const void *d_C, void *d_out, int reps, float *h_ms)
 {

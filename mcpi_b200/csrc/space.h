@@ -41,6 +41,10 @@ struct mcpi_space_s {
     int64_t nc = 0, nc1 = 0, nc2 = 0;
     int P = 0;
     cudaStream_t own = nullptr, stream = nullptr;
+    // host-buffer pipeline of mcpi_apply_h_host (created at its first call)
+    cudaStream_t s_h2d = nullptr, s_d2h = nullptr;
+    double2 *d_hin[2] = {nullptr, nullptr}, *d_hout[2] = {nullptr, nullptr};
+    cudaEvent_t ev_in[2] = {nullptr, nullptr}, ev_comp[2] = {nullptr, nullptr}, ev_out[2] = {nullptr, nullptr};
     uint32_t *d_W = nullptr;
     double *d_sq = nullptr;
     bool has_op = false;

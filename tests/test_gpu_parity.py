@@ -273,3 +273,25 @@ def test_gemm_and_csr_pair_kernels_agree(orc, N, M):
     Ho2, Hint2 = mc.lieb_integrals(M, 1.5)
     sp.set_integrals(Ho2, Hint2)
     assert rel(sp.apply_h(C).cpu().numpy(), orc.apply_h(N, M, C, Ho2, Hint2, mode=2)) <= TOL
+
+
+def test_apply_h_host_pipeline(orc):
+    # host-buffer pipeline: numpy and pinned torch states, repeated states, an
+    # odd count (the two device buffer pairs alternate), against the oracle
+    import torch
+    N, M = 7, 8
+    sp = _space(N, M)
+    _, Ho, Hint = mc.random_problem(N, M, 31)
+    sp.set_integrals(Ho, Hint)
+    states = [mc.random_problem(N, M, 40 + k)[0] for k in range(3)]
+    refs = [orc.apply_h(N, M, C, Ho, Hint, mode=2) for C in states]
+    order = [0, 1, 2, 1, 0]
+    ins = [states[k] for k in order[:3]] + [torch.from_numpy(states[k]).pin_memory() for k in order[3:]]
+    outs = [np.zeros(sp.nc, np.complex128) for _ in range(3)] + \
+           [torch.zeros(sp.nc, dtype=torch.complex128).pin_memory() for _ in range(2)]
+    sp.apply_h_host(ins, outs)
+    for k, o in zip(order, outs):
+        o = o.numpy() if hasattr(o, "numpy") else o
+        assert rel(o, refs[k]) <= TOL
+    assert sp.apply_h_host([], []) == []
+    sp.close()
