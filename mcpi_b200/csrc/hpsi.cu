@@ -34,6 +34,7 @@ constexpr int kT1 = 64;    // threads (= (N-2)-configurations) per block, kernel
 constexpr int kCsrStaged = 1024;   // pair-matrix nonzeros staged in shared memory
 constexpr int kT2 = 256;   // threads per block, kernel 2 (register form) and kernel 1 (momentum form)
 constexpr int kTC = 256;   // threads (= rows) per block, kernel 2 (shared-table form)
+constexpr int kCreateBatch = 8;   // E gathers issued together per thread, kernel 2 (shared-table form)
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
 {
@@ -765,7 +766,8 @@ __global__ void __launch_bounds__(kT2, 4) k_pair_create(Space sp, SpaceTables tb
 // and v_k - 1) live in shared-memory columns that only their thread touches,
 // so the pair loop needs few registers (no spills) and occupancy is set by
 // shared memory (17 bytes per orbital and row). Measured at N=16, M=10:
-// 0.198 ms, against 0.238 ms with two double tables, 0.248 ms for the register
+// 0.183 ms with the E gathers issued in groups of 8 (0.198 ms consumed one by
+// one, 0.186 ms in groups of 16), against 0.238 ms with two double tables, 0.248 ms for the register
 // form, 0.216 ms keeping only occupation bytes (square roots looked up per
 // pair), 0.21 ms forcing five blocks per SM (spills); staging each block's
 // contiguous E ranges in shared memory with TMA bulk copies (0.73 ms) or
@@ -824,21 +826,44 @@ __device__ __forceinline__ void create_smem_body(const Space &sp, const SpaceTab
     }
     const size_t stride = sp.nc2;
     if (!row) return;
+    // pairs p = pair_index(k, s) in order, in groups of kCreateBatch: all loads
+    // of a group are issued before any is consumed (E is read exactly once:
+    // streaming loads), so each thread keeps a group of gathers in flight
+    constexpr int NPR = M * (M + 1) / 2;
 #pragma unroll
-    for (int k = 0; k < M; ++k)
+    for (int p0 = 0; p0 < NPR; p0 += kCreateBatch) {
+        double cc[kCreateBatch];
+        double2 ee[kCreateBatch];
 #pragma unroll
-        for (int s = k; s < M; ++s) {
-            const double c = r1[k * kTC + t] * ((s == k) ? sq[vb[k * kTC + t]] : r1[s * kTC + t]);
-            const uint32_t mm = c != 0.0 ? Xr[k * kTC + t] - Yr[s * kTC + t] : 0u;
-            const double2 e = __ldg(E + pair_index(k, s, M) * stride + mm);
-            acc.x = fma(c, e.x, acc.x);
-            acc.y = fma(c, e.y, acc.y);
+        for (int j = 0; j < kCreateBatch; ++j) {
+            const int p = p0 + j;
+            if (p < NPR) {
+                int k = 0, rem = p;   // (k, s) of pair p, resolved at compile time
+#pragma unroll
+                for (int kk = 0; kk < M; ++kk)
+                    if (rem >= M - kk && k == kk) {
+                        rem -= M - kk;
+                        k = kk + 1;
+                    }
+                const int s = k + rem;
+                const double c = r1[k * kTC + t] * ((s == k) ? sq[vb[k * kTC + t]] : r1[s * kTC + t]);
+                const uint32_t mm = c != 0.0 ? Xr[k * kTC + t] - Yr[s * kTC + t] : 0u;
+                cc[j] = c;
+                ee[j] = __ldcs(E + (size_t)p * stride + mm);
+            }
         }
+#pragma unroll
+        for (int j = 0; j < kCreateBatch; ++j)
+            if (p0 + j < NPR) {
+                acc.x = fma(cc[j], ee[j].x, acc.x);
+                acc.y = fma(cc[j], ee[j].y, acc.y);
+            }
+    }
     out[i - row0] = acc;
 }
 
 template <int M>
-__global__ void __launch_bounds__(kTC) k_pair_create_smem(Space sp, SpaceTables tb, PairOp op,
+__global__ void __launch_bounds__(kTC, 4) k_pair_create_smem(Space sp, SpaceTables tb, PairOp op,
                                                           const double2 *__restrict__ psi,
                                                           const double2 *__restrict__ E,
                                                           double2 *__restrict__ out, uint32_t row0,
@@ -865,7 +890,7 @@ __global__ void __launch_bounds__(kT2, 3) k_batch_annihilate(const BatchMember *
 }
 
 template <int M>
-__global__ void __launch_bounds__(kTC) k_batch_create(const BatchMember *__restrict__ mem,
+__global__ void __launch_bounds__(kTC, 4) k_batch_create(const BatchMember *__restrict__ mem,
                                                       const int2 *__restrict__ work, int vec)
 {
     const int2 w = work[blockIdx.x];
