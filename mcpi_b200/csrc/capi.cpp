@@ -446,6 +446,8 @@ int mcpi_space_destroy(mcpi_space sp)
     cudaFree(sp->d_gram);
     cudaFree(sp->d_dot);
     cudaFree(sp->d_status);
+    cudaFree(sp->d_occ);
+    cudaFree(sp->d_occ2);
     if (sp->s_h2d) cudaStreamSynchronize(sp->s_h2d);
     if (sp->s_d2h) cudaStreamSynchronize(sp->s_d2h);
     for (int b = 0; b < 2; ++b) {
@@ -690,6 +692,28 @@ int mcpi_set_integrals(mcpi_space sp, const double *h_Ho, const double *h_Hint, 
     if (rc) return rc;
     sp->fwd.create_form = sp->adj.create_form = sp->create_form;
     sp->fwd.status = sp->adj.status = sp->d_status;
+    // packed occupations of the N- and (N-2)-space rows, read by the H.psi
+    // kernels instead of decoding each row index (8 bytes per configuration;
+    // skipped, and the kernels decode, when they do not fit 64 bits or memory
+    // is short)
+    const int bits = mcpi::occ_bits_for(sp->N, sp->M);
+    if (!sp->d_occ && bits && sp->N >= 2 && sp->nc2 > 0) {
+        const size_t b1 = sizeof(uint64_t) * (size_t)sp->nc, b2 = sizeof(uint64_t) * (size_t)sp->nc2;
+        if (cudaMalloc(&sp->d_occ, b1) == cudaSuccess && cudaMalloc(&sp->d_occ2, b2) == cudaSuccess) {
+            const mcpi::SpaceTables t{sp->d_W, sp->d_sq};
+            mcpi::Space s2 = sp->sp;
+            s2.N = sp->N - 2;
+            s2.nc = (uint32_t)sp->nc2;
+            CK(mcpi::launch_pack_occ(sp->sp, t, sp->d_occ, bits, sp->stream));
+            CK(mcpi::launch_pack_occ(s2, t, sp->d_occ2, bits, sp->stream));
+            sp->occ_bits = bits;
+        } else {
+            (void)cudaGetLastError();
+            cudaFree(sp->d_occ);
+            sp->d_occ = nullptr;
+            sp->d_occ2 = nullptr;
+        }
+    }
     sp->has_op = true;
     return MCPI_OK;
 }

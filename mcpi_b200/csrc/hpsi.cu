@@ -78,6 +78,27 @@ __device__ __forceinline__ void load_tables(const Space &sp, const SpaceTables &
     for (int x = threadIdx.x; x < sp.wstride; x += blockDim.x) sq[x] = tb.sq[x];
 }
 
+// Occupations v and prefix counts P of configuration idx of an n-particle
+// space: from the packed table when there is one, else by decoding the index.
+template <int M>
+__device__ __forceinline__ void occupations(const uint64_t *occ, int bits, uint32_t idx, int n, uint32_t ncn,
+                                            const uint32_t *W, int ws, int *v, int *P)
+{
+    if (occ) {
+        const uint64_t w = occ[idx];
+        const uint32_t mask = (1u << bits) - 1u;
+        int run = 0;
+#pragma unroll
+        for (int q = 0; q < M; ++q) {
+            v[q] = (int)((w >> (bits * q)) & mask);
+            run += v[q];
+            P[q] = run;
+        }
+    } else {
+        decode<M>(idx, n, ncn, W, ws, v, P);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // kernel 1: E[a][m] = sum_b Ht[a][b] c_b(m) psi[index(m + pair b)]
 // ---------------------------------------------------------------------------
@@ -110,7 +131,7 @@ __global__ void __launch_bounds__(kT1) k_pair_annihilate(Space sp, SpaceTables t
     const int ws = sp.wstride;
 
     int u[M], Q[M];
-    decode<M>(m, sp.N - 2, sp.nc2, W, ws, u, Q);
+    occupations<M>(tb.occ2, tb.occ_bits, m, sp.N - 2, sp.nc2, W, ws, u, Q);
     uint32_t B0[M], B1[M], B2[M];
     prefix_table<M>(Q, 0, W, ws, B0);
     prefix_table<M>(Q, 1, W, ws, B1);
@@ -199,13 +220,14 @@ struct GemmShape {
 // occupations u of the configuration are returned for the scaling once the
 // copies have landed. Configurations past nc2 get zero rows.
 template <int M, int kParts>
-__device__ __forceinline__ void gemm_gather(const Space &sp, const uint32_t *W, const double2 *__restrict__ psi,
-                                            double2 *D, uint32_t m, int cfg, int part, int (&u)[M])
+__device__ __forceinline__ void gemm_gather(const Space &sp, const SpaceTables &tb, const uint32_t *W,
+                                            const double2 *__restrict__ psi, double2 *D, uint32_t m, int cfg,
+                                            int part, int (&u)[M])
 {
     constexpr int P = M * (M + 1) / 2;
     if (m < sp.nc2) {
         int Q[M];
-        decode<M>(m, sp.N - 2, sp.nc2, W, sp.wstride, u, Q);
+        occupations<M>(tb.occ2, tb.occ_bits, m, sp.N - 2, sp.nc2, W, sp.wstride, u, Q);
         uint32_t B0[M], B1[M], B2[M];
         prefix_table<M>(Q, 0, W, sp.wstride, B0);
         prefix_table<M>(Q, 1, W, sp.wstride, B1);
@@ -370,7 +392,7 @@ __global__ void __launch_bounds__(kTG, M <= 10 ? 2 : 1)
     const int cfg = threadIdx.x % kGM, part = threadIdx.x / kGM;
     for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         int u[M];
-        gemm_gather<M, kParts>(sp, W, psi, D, tile * kGM + cfg, cfg, part, u);
+        gemm_gather<M, kParts>(sp, tb, W, psi, D, tile * kGM + cfg, cfg, part, u);
         asm volatile("cp.async.wait_group 0;\n" ::: "memory");
         gemm_scale<M, kParts>(sq, D, u, cfg, part);
         __syncthreads();
@@ -495,7 +517,7 @@ __global__ void __launch_bounds__(kTW, 1)
                 return;
             }
             int u[M];
-            gemm_gather<M, 1>(sp, W, psi, D, (blockIdx.x + i * gridDim.x) * kGM + cfg, cfg, 0, u);
+            gemm_gather<M, 1>(sp, tb, W, psi, D, (blockIdx.x + i * gridDim.x) * kGM + cfg, cfg, 0, u);
             if constexpr (CS) gemm_coeffs<M>(ct, nu, Cbuf + buf * PK * kGM, u, cfg);
             asm volatile("cp.async.wait_group 0;\n" ::: "memory");
             if constexpr (!CS) gemm_scale<M, 1>(sq, D, u, cfg, 0);
@@ -566,7 +588,7 @@ __global__ void __launch_bounds__(kT1b) k_pair_annihilate_blocks(Space sp, Space
     const int ws = sp.wstride;
     {
         int u[M], Q[M];
-        decode<M>(m, sp.N - 2, sp.nc2, W, ws, u, Q);
+        occupations<M>(tb.occ2, tb.occ_bits, m, sp.N - 2, sp.nc2, W, ws, u, Q);
         uint32_t B0[M], B1[M], B2[M];
         prefix_table<M>(Q, 0, W, ws, B0);
         prefix_table<M>(Q, 1, W, ws, B1);
@@ -640,7 +662,7 @@ __device__ __forceinline__ void annihilate_momentum_body(const Space &sp, const 
     if (m >= sp.nc2) return;
     const int ws = sp.wstride;
     int u[M], Q[M];
-    decode<M>(m, sp.N - 2, sp.nc2, W, ws, u, Q);
+    occupations<M>(tb.occ2, tb.occ_bits, m, sp.N - 2, sp.nc2, W, ws, u, Q);
     uint32_t B0[M], B1[M], B2[M];
     prefix_table<M>(Q, 0, W, ws, B0);
     prefix_table<M>(Q, 1, W, ws, B1);
@@ -717,7 +739,7 @@ __global__ void __launch_bounds__(kT2, 4) k_pair_create(Space sp, SpaceTables tb
     const int ws = sp.wstride;
 
     int v[M], P[M];
-    decode<M>(i, sp.N, sp.nc, W, ws, v, P);
+    occupations<M>(tb.occ, tb.occ_bits, i, sp.N, sp.nc, W, ws, v, P);
 
     double2 h1 = make_double2(0.0, 0.0);
 #pragma unroll
@@ -799,7 +821,7 @@ __device__ __forceinline__ void create_smem_body(const Space &sp, const SpaceTab
     double2 acc;
     {
         int v[M], P[M];
-        decode<M>(row ? i : 0u, sp.N, sp.nc, W, ws, v, P);
+        occupations<M>(tb.occ, tb.occ_bits, row ? i : (tb.occ ? row0 : 0u), sp.N, sp.nc, W, ws, v, P);
         double2 h1 = make_double2(0.0, 0.0);
 #pragma unroll
         for (int k = 0; k < M; ++k) {

@@ -49,7 +49,17 @@ struct BlockOp {
 struct SpaceTables {
     const uint32_t *W;      // (M-1) x wstride, W[i*ws + p] = C(p+i, i+1) mod 2^32
     const double *sq;       // sqrt(n), n = 0 .. N+2
+    // optional: occupations of every configuration of the space, occ_bits bits
+    // per orbital (orbital k in bits [k*occ_bits, (k+1)*occ_bits)); kernels that
+    // read it skip the index decode, null means decode
+    const uint64_t *occ = nullptr;
+    int occ_bits = 0;
+    const uint64_t *occ2 = nullptr;   // the same for the (N-2)-particle space (occ_bits bits)
 };
+// Bits per orbital of the packed occupation table of an N-particle space (0:
+// M orbitals do not fit in 64 bits).
+int occ_bits_for(int N, int M);
+cudaError_t launch_pack_occ(const Space &sp, const SpaceTables &tb, uint64_t *occ, int bits, cudaStream_t st);
 
 // H.psi : out = H psi. E is scratch of P * nc2 complex (unused when N < 2).
 // stages: bit 0 = kernel 1 (pair annihilation + pair matrix, writes E),

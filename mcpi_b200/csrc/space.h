@@ -58,5 +58,8 @@ struct mcpi_space_s {
     int kernel_choice = 0;           // 2: skip the momentum-block kernel
     bool no_gemm = false;            // general pair matrices use the CSR kernel (MCPI_OPT_NO_GEMM_KERNEL)
     int create_form = 0;            // pair-creation kernel form (MCPI_OPT_CREATE_FORM)
-    mcpi::SpaceTables tables() const { return mcpi::SpaceTables{d_W, d_sq}; }
+    uint64_t *d_occ = nullptr;       // packed occupations of the space's rows (built by mcpi_set_integrals)
+    uint64_t *d_occ2 = nullptr;      // the same for the (N-2)-particle space
+    int occ_bits = 0;
+    mcpi::SpaceTables tables() const { return mcpi::SpaceTables{d_W, d_sq, d_occ, occ_bits, d_occ2}; }
 };

@@ -41,6 +41,23 @@ __global__ void k_focks(Space sp, SpaceTables tb, int32_t *__restrict__ IF)
     for (int j = 0; j < M; ++j) IF[(size_t)i * M + j] = v[j];
 }
 
+// Packed occupations (bits per orbital) of every configuration, for kernels
+// that would otherwise decode their row index.
+template <int M>
+__global__ void k_pack_occ(Space sp, SpaceTables tb, int bits, uint64_t *__restrict__ occ)
+{
+    extern __shared__ uint32_t W[];
+    load_w(sp, tb, W);
+    const uint32_t i = blockIdx.x * kThreads + threadIdx.x;
+    if (i >= sp.nc) return;
+    int v[M], P[M];
+    decode<M>(i, sp.N, sp.nc, W, sp.wstride, v, P);
+    uint64_t w = 0;
+#pragma unroll
+    for (int j = 0; j < M; ++j) w |= (uint64_t)v[j] << (bits * j);
+    occ[i] = w;
+}
+
 template <int M>
 __global__ void k_one_one(Space sp, SpaceTables tb, int32_t *__restrict__ Map)
 {
@@ -178,6 +195,15 @@ struct RunFocks {
 };
 
 template <int M>
+struct RunPackOcc {
+    static cudaError_t run(Space sp, SpaceTables tb, int bits, uint64_t *occ, cudaStream_t st)
+    {
+        k_pack_occ<M><<<gridn(sp), kThreads, wbytes(sp), st>>>(sp, tb, bits, occ);
+        return cudaGetLastError();
+    }
+};
+
+template <int M>
 struct RunOneOne {
     static cudaError_t run(Space sp, SpaceTables tb, int32_t *Map, cudaStream_t st)
     {
@@ -210,6 +236,19 @@ struct RunTwoMap {
 cudaError_t launch_focks(const Space &sp, const SpaceTables &tb, int32_t *IF, cudaStream_t st)
 {
     return by_m<RunFocks>(sp.M, sp, tb, IF, st);
+}
+
+int occ_bits_for(int N, int M)
+{
+    int b = 1;
+    while ((1 << b) <= N) ++b;
+    return M * b <= 64 ? b : 0;
+}
+
+cudaError_t launch_pack_occ(const Space &sp, const SpaceTables &tb, uint64_t *occ, int bits, cudaStream_t st)
+{
+    if (bits <= 0 || sp.M * bits > 64) return cudaErrorInvalidValue;
+    return by_m<RunPackOcc>(sp.M, sp, tb, bits, occ, st);
 }
 
 cudaError_t launch_one_one_map(const Space &sp, const SpaceTables &tb, int32_t *Map, cudaStream_t st)
