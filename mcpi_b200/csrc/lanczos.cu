@@ -185,6 +185,8 @@ __global__ void k_multidot_finish(const double2 *__restrict__ partial, int nblk,
     if (lane == 0) coef[j] = acc;
 }
 
+constexpr int kUpdBatch = 8;   // basis entries in flight per thread in k_update
+
 // Pass 2: r = (r - alpha vcur) - sum_j V_j coef_j ; partial of |r|^2
 __global__ void __launch_bounds__(kThreads) k_update(const double2 *__restrict__ V, int nvec,
                                                      int64_t n, double2 *__restrict__ r,
@@ -204,7 +206,20 @@ __global__ void __launch_bounds__(kThreads) k_update(const double2 *__restrict__
          x += (int64_t)gridDim.x * kThreads) {
         const double2 y = r[x], v = vcur[x];
         double2 u = make_double2(y.x - (a.x * v.x - a.y * v.y), y.y - (a.x * v.y + a.y * v.x));
-        for (int j = 0; j < nvec; ++j) {
+        // kUpdBatch basis entries loaded together, then subtracted in order j
+        int j = 0;
+        for (; j + kUpdBatch <= nvec; j += kUpdBatch) {
+            double2 p[kUpdBatch];
+#pragma unroll
+            for (int q = 0; q < kUpdBatch; ++q) p[q] = V[(size_t)(j + q) * n + x];
+#pragma unroll
+            for (int q = 0; q < kUpdBatch; ++q) {
+                const double2 c = cs[j + q];
+                u.x -= p[q].x * c.x - p[q].y * c.y;
+                u.y -= p[q].x * c.y + p[q].y * c.x;
+            }
+        }
+        for (; j < nvec; ++j) {
             const double2 p = V[(size_t)j * n + x], c = cs[j];
             u.x -= p.x * c.x - p.y * c.y;
             u.y -= p.x * c.y + p.y * c.x;
