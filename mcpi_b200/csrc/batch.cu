@@ -401,6 +401,8 @@ int mcpi_batch_create(int count, const int *N, const int *M, int lm, int device,
         bm.E = reinterpret_cast<double2 *>(b->arena + off_E[m]);
         bm.r = z.r;
         bm.done = z.done;
+        bm.occ = bm.occ2 = nullptr;
+        bm.occ_bits = 0;
     }
     // work tables: vector tiles of every member, H.psi blocks grouped by M
     std::vector<int2> vwork;
@@ -489,6 +491,9 @@ int mcpi_batch_set_integrals(mcpi_batch b, int member, const double *h_Ho, const
     bm.hblk = s->fwd.hblk;
     bm.nh = s->fwd.nhblk;
     bm.hdiag = s->fwd.hdiag;
+    bm.occ = s->d_occ;
+    bm.occ2 = s->d_occ2;
+    bm.occ_bits = s->occ_bits;
     b->ready[member] |= 1;
     if (cudaMemcpy(b->d_mem + member, &bm, sizeof(BatchMember), cudaMemcpyHostToDevice) != cudaSuccess)
         return bfail(MCPI_ERR_CUDA, "member upload failed");

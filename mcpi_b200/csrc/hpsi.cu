@@ -907,7 +907,7 @@ __global__ void __launch_bounds__(kT2, 3) k_batch_annihilate(const BatchMember *
     const int2 w = work[blockIdx.x];
     const BatchMember &b = mem[w.x];
     if (*b.done) return;
-    annihilate_momentum_body<M>(b.sp, SpaceTables{b.W, b.sq}, b.hblk, b.nh,
+    annihilate_momentum_body<M>(b.sp, SpaceTables{b.W, b.sq, b.occ, b.occ_bits, b.occ2}, b.hblk, b.nh,
                                 b.lvec + (size_t)vec * b.sp.nc, b.E, (uint32_t)w.y);
 }
 
@@ -918,7 +918,7 @@ __global__ void __launch_bounds__(kTC, 4) k_batch_create(const BatchMember *__re
     const int2 w = work[blockIdx.x];
     const BatchMember &b = mem[w.x];
     if (*b.done) return;
-    create_smem_body<M>(b.sp, SpaceTables{b.W, b.sq}, b.hdiag, b.lvec + (size_t)vec * b.sp.nc, b.E,
+    create_smem_body<M>(b.sp, SpaceTables{b.W, b.sq, b.occ, b.occ_bits, b.occ2}, b.hdiag, b.lvec + (size_t)vec * b.sp.nc, b.E,
                         b.r, (uint32_t)w.y, 0u, b.sp.nc);
 }
 

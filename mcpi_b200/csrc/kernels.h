@@ -85,6 +85,9 @@ struct BatchMember {
     double2 *E;              // P x nc2 intermediate
     double2 *r;              // H.psi output (the Lanczos residual)
     const int *done;         // this member's breakdown flag
+    const uint64_t *occ;     // packed occupations of the N and N-2 spaces (or null: decode)
+    const uint64_t *occ2;
+    int occ_bits;
 };
 
 // Batched H.psi for the members of one M: work1 / work2 list (member,
