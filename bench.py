@@ -183,6 +183,7 @@ def run_batch(mc, torch, device, iters=120):
     E, it = b.run()
     t_batch = time.perf_counter() - t0
     arena = b.arena_bytes()
+    tile, tune_ms = b.schedule()
     b.close()
     spaces = []
     for k, (n, m, g) in enumerate(members):
@@ -204,7 +205,8 @@ def run_batch(mc, torch, device, iters=120):
             "seconds": t_batch, "sequential_solves_per_s": len(members) / t_seq,
             "sequential_seconds": t_seq, "speedup_vs_sequential": t_seq / t_batch,
             "max_rel_dE0_vs_sequential": dE, "steps_done_min": int(it.min()),
-            "nc_min": min(ncs), "nc_max": max(ncs), "arena_gb": arena / 1e9}
+            "nc_min": min(ncs), "nc_max": max(ncs), "arena_gb": arena / 1e9,
+            "tile_rows": tile, "tile_probe_ms": {str(t): float(x) for t, x in zip((512, 1024, 2048), tune_ms)}}
 
 
 def run_large(mc, torch, device):

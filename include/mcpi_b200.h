@@ -206,6 +206,16 @@ MCPI_API int mcpi_batch_set_start(mcpi_batch b, int member, const void *C);
  * returns each member's lowest eigenvalue and Lanczos step count. */
 MCPI_API int mcpi_batch_run(mcpi_batch b, double *h_E0, int *h_iters);
 MCPI_API int mcpi_batch_arena_bytes(mcpi_batch b, size_t *bytes);
+/* Tile schedule of the batch's vector stages (rows of one member per work tile:
+ * 512, 1024 or 2048). 0 (the default) lets the first mcpi_batch_run time one
+ * Lanczos step's vector stages with each tile on this batch's own arena and
+ * keep the fastest (the autotuner); a fixed value pins it, e.g. to reproduce
+ * results bit for bit across processes (the tile sets the reduction order).
+ * Only before the first mcpi_batch_run. No reference counterpart. */
+MCPI_API int mcpi_batch_set_schedule(mcpi_batch b, int tile_rows);
+/* The tile in use (0 before the first run) and, when it was autotuned, the
+ * probe time of each candidate 512 / 1024 / 2048 in h_ms[0..2] (ms; may be NULL). */
+MCPI_API int mcpi_batch_schedule(mcpi_batch b, int *tile_rows, float *h_ms);
 MCPI_API int mcpi_batch_destroy(mcpi_batch b);
 
 /* ---- model inputs ------------------------------------------------------------ */

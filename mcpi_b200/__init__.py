@@ -94,6 +94,8 @@ def lib():
         "mcpi_batch_set_start": (i, [_vp, i, _vp]),
         "mcpi_batch_run": (i, [_vp, _vp, _vp]),
         "mcpi_batch_arena_bytes": (i, [_vp, ct.POINTER(ct.c_size_t)]),
+        "mcpi_batch_set_schedule": (i, [_vp, i]),
+        "mcpi_batch_schedule": (i, [_vp, ct.POINTER(ct.c_int), _vp]),
         "mcpi_batch_destroy": (i, [_vp]),
     }
     for name, (res, args) in sig.items():
@@ -437,6 +439,19 @@ class Batch:
         v = ct.c_size_t(0)
         _check(lib().mcpi_batch_arena_bytes(self._h, ct.byref(v)))
         return v.value
+
+    def set_schedule(self, tile_rows: int):
+        """Pin the vector-stage tile (512, 1024, 2048) or 0 to autotune at the
+        first run (before the first run only)."""
+        _check(lib().mcpi_batch_set_schedule(self._h, int(tile_rows)))
+
+    def schedule(self):
+        """(tile rows in use or 0 before the first run, probe ms of the
+        candidates 512 / 1024 / 2048 when autotuned, else zeros)."""
+        t = ct.c_int(0)
+        ms = np.zeros(3, np.float32)
+        _check(lib().mcpi_batch_schedule(self._h, ct.byref(t), _np_ptr(ms)))
+        return t.value, ms
 
     def close(self):
         if getattr(self, "_h", None):

@@ -39,14 +39,16 @@ struct BatchLz {
     int *done;         // 1
     int *iters;        // 1
     double2 *coef;     // lm
-    double2 *part;     // (lm + 1) * ntiles partial sums
-    int ntiles;        // ceil(nc / kTileRows)
+    double2 *part;     // (lm + 1) * ceil(nc / kTileMin) partial sums (room for the smallest tile)
+    int ntiles;        // ceil(nc / tile) for the batch's tile
 };
 
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kTileRows = 2048;
+// rows per work tile of the vector stages: the autotuner picks one of these
+constexpr int kTileCands[3] = {512, 1024, 2048};
+constexpr int kTileMin = 512;
 
 __device__ __forceinline__ double2 warp_sum2(double2 v)
 {
@@ -90,13 +92,14 @@ __global__ void kb_reset(BatchLz *L, int nmem, int lm)
 }
 
 // partial of <V_a, r> over one tile; with beta_i set, r -= beta_i V_prev first
+template <int T>
 __global__ void kb_axpy_dot(BatchLz *L, const int2 *__restrict__ work, int i)
 {
     const int2 w = work[blockIdx.x];
     BatchLz &b = L[w.x];
     if (*b.done) return;
-    const int64_t r0 = (int64_t)w.y * kTileRows;
-    const int64_t r1 = min(b.nc, r0 + kTileRows);
+    const int64_t r0 = (int64_t)w.y * T;
+    const int64_t r1 = min(b.nc, r0 + T);
     const double2 *va = b.V + (size_t)(i + 1) * b.nc;
     const double2 *vp = i >= 0 ? b.V + (size_t)i * b.nc : nullptr;
     const double bi = i >= 0 ? b.beta[i] : 0.0;
@@ -132,15 +135,16 @@ __global__ void kb_sum_alpha(BatchLz *L, int k)
 }
 
 // part[j * ntiles + tile] = <V_j, r - alpha_cur V_cur> over the tile, j < nvec
+template <int T>
 __global__ void __launch_bounds__(kThreads) kb_multidot(BatchLz *L, const int2 *__restrict__ work,
                                                         int cur, int nvec)
 {
-    __shared__ double2 xs[kTileRows];
+    __shared__ double2 xs[T];
     const int2 w = work[blockIdx.x];
     BatchLz &b = L[w.x];
     if (*b.done) return;
-    const int64_t r0 = (int64_t)w.y * kTileRows;
-    const int rows = (int)min((int64_t)kTileRows, b.nc - r0);
+    const int64_t r0 = (int64_t)w.y * T;
+    const int rows = (int)min((int64_t)T, b.nc - r0);
     const double2 a = b.alpha[cur];
     const double2 *vc = b.V + (size_t)cur * b.nc + r0;
     for (int t = threadIdx.x; t < rows; t += kThreads) {
@@ -181,6 +185,7 @@ __global__ void kb_coef(BatchLz *L, int nvec)
 }
 
 // r = (r - alpha_cur V_cur) - sum_{j<nvec} coef_j V_j ; part[tile] = |r|^2 over the tile
+template <int T>
 __global__ void __launch_bounds__(kThreads) kb_update(BatchLz *L, const int2 *__restrict__ work,
                                                       int cur, int nvec)
 {
@@ -190,8 +195,8 @@ __global__ void __launch_bounds__(kThreads) kb_update(BatchLz *L, const int2 *__
     if (*b.done) return;
     for (int j = threadIdx.x; j < nvec; j += kThreads) cs[j] = b.coef[j];
     __syncthreads();
-    const int64_t r0 = (int64_t)w.y * kTileRows;
-    const int64_t r1 = min(b.nc, r0 + kTileRows);
+    const int64_t r0 = (int64_t)w.y * T;
+    const int64_t r1 = min(b.nc, r0 + T);
     const double2 a = b.alpha[cur];
     const double2 *vc = b.V + (size_t)cur * b.nc;
     double acc = 0.0;
@@ -229,13 +234,14 @@ __global__ void kb_beta(BatchLz *L, int i, double tol)
     }
 }
 
+template <int T>
 __global__ void kb_scale(BatchLz *L, const int2 *__restrict__ work, int i)
 {
     const int2 w = work[blockIdx.x];
     BatchLz &b = L[w.x];
     if (*b.done) return;
-    const int64_t r0 = (int64_t)w.y * kTileRows;
-    const int64_t r1 = min(b.nc, r0 + kTileRows);
+    const int64_t r0 = (int64_t)w.y * T;
+    const int64_t r1 = min(b.nc, r0 + T);
     const double bi = b.beta[i];
     double2 *vn = b.V + (size_t)(i + 1) * b.nc;
     for (int64_t x = r0 + threadIdx.x; x < r1; x += kThreads) {
@@ -302,8 +308,11 @@ struct mcpi_batch_s {
     char *meta = nullptr;   // device copies of lz, mem, work tables, results
     BatchLz *d_lz = nullptr;
     BatchMember *d_mem = nullptr;
-    int2 *d_vwork = nullptr;
+    int2 *d_vwork = nullptr;   // room for the smallest tile's work table
     int nvwork = 0;
+    int tile = 0;              // rows per vector-stage tile (0: autotune at the first run)
+    bool tuned = false;
+    float tune_ms[3] = {0.f, 0.f, 0.f};   // probe time of each candidate tile
     struct Group {
         int M;
         int2 *w1, *w2;
@@ -357,7 +366,7 @@ int mcpi_batch_create(int count, const int *N, const int *M, int lm, int device,
         if (rc) return cleanup(rc, std::string("member space: ") + mcpi_last_error());
         const mcpi_space_s *s = b->spaces[m];
         const int64_t nc = s->nc;
-        const int ntiles = (int)((nc + mcpi::kTileRows - 1) / mcpi::kTileRows);
+        const int ntiles = (int)((nc + mcpi::kTileMin - 1) / mcpi::kTileMin);   // room for any tile
         b->lz[m].nc = nc;
         b->lz[m].ntiles = ntiles;
         off_V[m] = tot;
@@ -386,7 +395,7 @@ int mcpi_batch_create(int count, const int *N, const int *M, int lm, int device,
         z.alpha = reinterpret_cast<double2 *>(st);
         z.coef = z.alpha + lm;
         z.part = z.coef + lm;
-        z.beta = reinterpret_cast<double *>(z.part + (size_t)(lm + 1) * z.ntiles);
+        z.beta = reinterpret_cast<double *>(z.part + (size_t)(lm + 1) * z.ntiles);   // ntiles for kTileMin here
         z.maxbeta = z.beta + lm;
         z.done = reinterpret_cast<int *>(z.maxbeta + 1);
         z.iters = z.done + 1;
@@ -510,7 +519,27 @@ int mcpi_batch_set_start(mcpi_batch b, int member, const void *C)
     return MCPI_OK;
 }
 
-static cudaError_t enqueue_solve(mcpi_batch b)
+}  // extern "C"
+
+// Rows per vector-stage tile: per-member tile counts and the (member, tile)
+// work table of every vector stage follow it.
+static cudaError_t set_tile(mcpi_batch b, int T)
+{
+    std::vector<int2> vwork;
+    for (int m = 0; m < b->count; ++m) {
+        b->lz[m].ntiles = (int)((b->lz[m].nc + T - 1) / T);
+        for (int t = 0; t < b->lz[m].ntiles; ++t) vwork.push_back(make_int2(m, t));
+    }
+    cudaError_t e = cudaMemcpy(b->d_lz, b->lz.data(), sizeof(BatchLz) * b->count, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(b->d_vwork, vwork.data(), sizeof(int2) * vwork.size(), cudaMemcpyHostToDevice);
+    b->nvwork = (int)vwork.size();
+    b->tile = T;
+    return e;
+}
+
+template <int T>
+static cudaError_t enqueue_solve_t(mcpi_batch b)
 {
     cudaStream_t st = b->stream;
     const int lm = b->lm, nm = b->count;
@@ -530,23 +559,105 @@ static cudaError_t enqueue_solve(mcpi_batch b)
     const int nw = b->nvwork;
     e = hpsi(0);
     if (e != cudaSuccess) return e;
-    mcpi::kb_axpy_dot<<<nw, mcpi::kThreads, 0, st>>>(b->d_lz, b->d_vwork, -1);
+    mcpi::kb_axpy_dot<T><<<nw, mcpi::kThreads, 0, st>>>(b->d_lz, b->d_vwork, -1);
     mcpi::kb_sum_alpha<<<nm, mcpi::kThreads, 0, st>>>(b->d_lz, 0);
-    mcpi::kb_update<<<nw, mcpi::kThreads, 0, st>>>(b->d_lz, b->d_vwork, 0, 0);
+    mcpi::kb_update<T><<<nw, mcpi::kThreads, 0, st>>>(b->d_lz, b->d_vwork, 0, 0);
     for (int i = 0; i < lm - 1; ++i) {
         mcpi::kb_beta<<<nm, mcpi::kThreads, 0, st>>>(b->d_lz, i, 1e-15);
-        mcpi::kb_scale<<<nw, mcpi::kThreads, 0, st>>>(b->d_lz, b->d_vwork, i);
+        mcpi::kb_scale<T><<<nw, mcpi::kThreads, 0, st>>>(b->d_lz, b->d_vwork, i);
         e = hpsi(i + 1);
         if (e != cudaSuccess) return e;
-        mcpi::kb_axpy_dot<<<nw, mcpi::kThreads, 0, st>>>(b->d_lz, b->d_vwork, i);
+        mcpi::kb_axpy_dot<T><<<nw, mcpi::kThreads, 0, st>>>(b->d_lz, b->d_vwork, i);
         mcpi::kb_sum_alpha<<<nm, mcpi::kThreads, 0, st>>>(b->d_lz, i + 1);
-        mcpi::kb_multidot<<<nw, mcpi::kThreads, 0, st>>>(b->d_lz, b->d_vwork, i + 1, i + 2);
+        mcpi::kb_multidot<T><<<nw, mcpi::kThreads, 0, st>>>(b->d_lz, b->d_vwork, i + 1, i + 2);
         mcpi::kb_coef<<<nm, mcpi::kThreads, 0, st>>>(b->d_lz, i + 2);
-        mcpi::kb_update<<<nw, mcpi::kThreads, sizeof(double2) * (i + 2), st>>>(b->d_lz, b->d_vwork, i + 1,
-                                                                                 i + 2);
+        mcpi::kb_update<T><<<nw, mcpi::kThreads, sizeof(double2) * (i + 2), st>>>(b->d_lz, b->d_vwork, i + 1,
+                                                                                    i + 2);
     }
     mcpi::kb_eig<<<(nm + 127) / 128, 128, 0, st>>>(b->d_lz, nm, b->d_E0, b->d_iters);
     return cudaGetLastError();
+}
+
+static cudaError_t enqueue_solve(mcpi_batch b)
+{
+    switch (b->tile) {
+    case 512: return enqueue_solve_t<512>(b);
+    case 1024: return enqueue_solve_t<1024>(b);
+    case 2048: return enqueue_solve_t<2048>(b);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+// One Lanczos step's vector stages at half the basis size (r -= beta v with the
+// alpha dot, the two reorthogonalisation passes, the scaling), on this batch's
+// own arena; the solve that follows re-initialises everything they touch.
+template <int T>
+static cudaError_t probe_tile(mcpi_batch b, int nvec)
+{
+    cudaStream_t st = b->stream;
+    const int nw = b->nvwork;
+    mcpi::kb_axpy_dot<T><<<nw, mcpi::kThreads, 0, st>>>(b->d_lz, b->d_vwork, nvec - 2);
+    mcpi::kb_multidot<T><<<nw, mcpi::kThreads, 0, st>>>(b->d_lz, b->d_vwork, nvec - 1, nvec);
+    mcpi::kb_update<T><<<nw, mcpi::kThreads, sizeof(double2) * nvec, st>>>(b->d_lz, b->d_vwork, nvec - 1, nvec);
+    mcpi::kb_scale<T><<<nw, mcpi::kThreads, 0, st>>>(b->d_lz, b->d_vwork, nvec - 2);
+    return cudaGetLastError();
+}
+
+// The autotuner: times the vector stages with each candidate tile (CUDA
+// events, best of three after a warm-up) and keeps the fastest.
+static cudaError_t autotune(mcpi_batch b)
+{
+    const int nvec = b->lm / 2 > 2 ? b->lm / 2 : 2;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaError_t e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    int best = -1;
+    for (int c = 0; c < 3 && e == cudaSuccess; ++c) {
+        const int T = mcpi::kTileCands[c];
+        e = set_tile(b, T);
+        if (e != cudaSuccess) break;
+        mcpi::kb_reset<<<(b->count + 127) / 128, 128, 0, b->stream>>>(b->d_lz, b->count, b->lm);
+        float ms = 1e30f;
+        for (int rep = 0; rep < 4 && e == cudaSuccess; ++rep) {
+            e = cudaEventRecord(e0, b->stream);
+            if (e == cudaSuccess)
+                e = T == 512 ? probe_tile<512>(b, nvec) : T == 1024 ? probe_tile<1024>(b, nvec) : probe_tile<2048>(b, nvec);
+            if (e == cudaSuccess) e = cudaEventRecord(e1, b->stream);
+            if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+            float t = 0.f;
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&t, e0, e1);
+            if (rep > 0 && t < ms) ms = t;   // the first repetition warms up
+        }
+        b->tune_ms[c] = ms;
+        if (best < 0 || ms < b->tune_ms[best]) best = c;
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (e == cudaSuccess) e = set_tile(b, mcpi::kTileCands[best]);
+    b->tuned = e == cudaSuccess;
+    return e;
+}
+
+extern "C" {
+
+int mcpi_batch_set_schedule(mcpi_batch b, int tile_rows)
+{
+    if (!b) return bfail(MCPI_ERR_ARG, "null batch");
+    if (b->exec) return bfail(MCPI_ERR_STATE, "mcpi_batch_set_schedule: the solve has already been captured");
+    if (tile_rows != 0 && tile_rows != 512 && tile_rows != 1024 && tile_rows != 2048)
+        return bfail(MCPI_ERR_ARG, "mcpi_batch_set_schedule: tile_rows must be 0, 512, 1024 or 2048");
+    b->tile = tile_rows;
+    b->tuned = false;
+    return MCPI_OK;
+}
+
+int mcpi_batch_schedule(mcpi_batch b, int *tile_rows, float *h_ms)
+{
+    if (!b) return bfail(MCPI_ERR_ARG, "null batch");
+    if (tile_rows) *tile_rows = b->exec ? b->tile : 0;
+    if (h_ms)
+        for (int c = 0; c < 3; ++c) h_ms[c] = b->tuned ? b->tune_ms[c] : 0.f;
+    return MCPI_OK;
 }
 
 int mcpi_batch_run(mcpi_batch b, double *h_E0, int *h_iters)
@@ -557,6 +668,8 @@ int mcpi_batch_run(mcpi_batch b, double *h_E0, int *h_iters)
     if (cudaSetDevice(b->device) != cudaSuccess) return bfail(MCPI_ERR_CUDA, "cudaSetDevice failed");
     cudaError_t e = cudaSuccess;
     if (!b->exec) {
+        e = b->tile == 0 ? autotune(b) : set_tile(b, b->tile);
+        if (e != cudaSuccess) return bfail(MCPI_ERR_CUDA, std::string("batch schedule: ") + cudaGetErrorString(e));
         e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
         if (e == cudaSuccess) {
             cudaError_t q = enqueue_solve(b);

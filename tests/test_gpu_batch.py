@@ -60,3 +60,36 @@ def test_batch_masks_a_breakdown():
     sp.set_integrals(*mc.lieb_integrals(7, 3.0))
     Es, _, its = sp.ground(C1, 20)
     assert it[1] == its == 20 and abs(E[1] - Es) <= 1e-10 * abs(Es)
+
+
+def test_batch_schedules_agree():
+    # every tile schedule gives the single-solve eigenvalues; the autotuner picks
+    # one of the candidates and reports a probe time for each
+    members = [(7, 9), (5, 11), (9, 7), (12, 7)]
+    gs = [1.5, 20.0, 0.3, 5.0]
+    lm = 30
+    starts = [_start(mc.nc_of(N, M), 200 + k) for k, (N, M) in enumerate(members)]
+    ref = []
+    for k, ((N, M), g) in enumerate(zip(members, gs)):
+        sp = mc.FockSpace(N, M)
+        sp.set_integrals(*mc.lieb_integrals(M, g))
+        ref.append(sp.ground(starts[k], lm)[0])
+    for tile in (512, 1024, 2048, 0):
+        b = mc.Batch(members, lm)
+        for k, ((N, M), g) in enumerate(zip(members, gs)):
+            b.set_integrals(k, *mc.lieb_integrals(M, g))
+            b.set_start(k, starts[k])
+        b.set_schedule(tile)
+        assert b.schedule()[0] == 0
+        E, _ = b.run()
+        used, ms = b.schedule()
+        assert used == (tile if tile else used) and used in (512, 1024, 2048)
+        if tile == 0:
+            assert np.all(ms > 0) and ms[(512, 1024, 2048).index(used)] == ms.min()
+        else:
+            assert np.all(ms == 0)
+        with pytest.raises(mc.MCPIError):
+            b.set_schedule(512)            # the solve is captured
+        for k in range(len(members)):
+            assert abs(E[k] - ref[k]) <= 1e-10 * max(1.0, abs(ref[k])), (tile, k, E[k], ref[k])
+        b.close()
