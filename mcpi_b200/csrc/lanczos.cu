@@ -14,7 +14,7 @@
 // Reductions go through per-block partials summed in block order by a single
 // block, so results are bitwise reproducible run to run. The two passes of the
 // reorthogonalisation read the Krylov basis once each (HBM bound, the dominant
-// Lanczos cost beside H.psi): pass 1 stages a 2048-row slice of
+// Lanczos cost beside H.psi): pass 1 stages a 1024-row slice of
 // x = r - alpha v_{i+1} in shared memory and lets each warp stream one basis
 // vector over it; pass 2 updates r row by row in the reference's per-element
 // order (x - v_0 c_0 - v_1 c_1 - ...) and emits the norm partials of the next
@@ -28,7 +28,7 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kParts = 592;          // blocks of the fixed-size reductions (4 x 148 SMs)
-constexpr int kSlice = 2048;         // rows per block in reorthogonalisation pass 1
+constexpr int kSlice = 1024;         // rows per block in reorthogonalisation pass 1
 
 __device__ __forceinline__ double2 cmulc(double2 a, double2 b)  // conj(a) * b
 {
