@@ -75,6 +75,15 @@ MCPI_API int mcpi_space_sync(mcpi_space sp);
  * compressed-row kernel instead of the register-tiled dense product (which is
  * otherwise chosen for M <= 12). Takes effect at the next mcpi_set_integrals. */
 #define MCPI_OPT_NO_GEMM_KERNEL 4
+/* MCPI_OPT_WAIT_LIMIT_KCYCLES (>= 0): limit, in thousands of SM cycles, of
+ * each bounded wait inside the warp-specialised dense-product kernel (0, the
+ * default: about two seconds). A wait that runs out makes the kernel return
+ * and the next synchronising call report MCPI_ERR_TIMEOUT. */
+#define MCPI_OPT_WAIT_LIMIT_KCYCLES 5
+/* MCPI_OPT_TEST_STALL_GATHER (0/1): for testing the timeout path only — the
+ * dense-product kernel's gather warps deliver no tile, so its product warps'
+ * waits run out (results are invalid while it is set). */
+#define MCPI_OPT_TEST_STALL_GATHER 6
 MCPI_API int mcpi_space_set_option(mcpi_space sp, int option, int value);
 MCPI_API int mcpi_space_dims(mcpi_space sp, int *N, int *M, int64_t *nc);
 /* Device memory on the space's device, and a synchronous copy in any direction

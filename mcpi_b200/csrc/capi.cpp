@@ -478,6 +478,15 @@ int mcpi_space_set_option(mcpi_space sp, int option, int value)
     case MCPI_OPT_DENSE_PAIR_KERNEL: sp->dense_only = value != 0; return MCPI_OK;
     case MCPI_OPT_NO_MOMENTUM_KERNEL: sp->kernel_choice = value ? 2 : 0; return MCPI_OK;
     case MCPI_OPT_NO_GEMM_KERNEL: sp->no_gemm = value != 0; return MCPI_OK;
+    case MCPI_OPT_WAIT_LIMIT_KCYCLES:
+        if (value < 0) return fail(MCPI_ERR_ARG, "wait limit must be >= 0");
+        sp->wait_cycles = 1000LL * value;
+        sp->fwd.wait_cycles = sp->adj.wait_cycles = sp->wait_cycles;
+        return MCPI_OK;
+    case MCPI_OPT_TEST_STALL_GATHER:
+        sp->test_stall = value != 0;
+        sp->fwd.test_stall = sp->adj.test_stall = sp->test_stall;
+        return MCPI_OK;
     case MCPI_OPT_CREATE_FORM:
         sp->create_form = value;
         sp->fwd.create_form = sp->adj.create_form = value;
@@ -692,6 +701,8 @@ int mcpi_set_integrals(mcpi_space sp, const double *h_Ho, const double *h_Hint, 
     if (rc) return rc;
     sp->fwd.create_form = sp->adj.create_form = sp->create_form;
     sp->fwd.status = sp->adj.status = sp->d_status;
+    sp->fwd.wait_cycles = sp->adj.wait_cycles = sp->wait_cycles;
+    sp->fwd.test_stall = sp->adj.test_stall = sp->test_stall;
     // packed occupations of the N- and (N-2)-space rows, read by the H.psi
     // kernels instead of decoding each row index (8 bytes per configuration;
     // skipped, and the kernels decode, when they do not fit 64 bits or memory

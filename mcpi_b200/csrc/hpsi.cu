@@ -442,8 +442,8 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar)
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_addr(bar)) : "memory");
 }
 
-// true once the phase of the given parity has completed; false after kWaitCycles
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
+// true once the phase of the given parity has completed; false after limit cycles
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long long limit)
 {
     const long long t0 = clock64();
     for (;;) {
@@ -458,7 +458,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
             : "r"(smem_addr(bar)), "r"(parity)
             : "memory");
         if (ok) return true;
-        if (clock64() - t0 > kWaitCycles) return false;
+        if (clock64() - t0 > limit) return false;
     }
 }
 
@@ -466,8 +466,9 @@ template <int M, int NS, bool CS>
 __global__ void __launch_bounds__(kTW, 1)
     k_pair_annihilate_gemm_ws(Space sp, SpaceTables tb, const double2 *__restrict__ H,
                               const double2 *__restrict__ psi, double2 *__restrict__ E, uint32_t ntiles,
-                              int *status)
+                              int *status, long long wait_cycles, int test_stall)
 {
+    const long long limit = wait_cycles > 0 ? wait_cycles : kWaitCycles;
     using G = GemmShape<M>;
     constexpr int P = G::P, PA = G::PA, PK = G::PK, HS = G::HS;
     constexpr int kProdThreads = 2 * kTG;
@@ -512,7 +513,8 @@ __global__ void __launch_bounds__(kTW, 1)
         for (uint32_t i = grp; i < ntb; i += kGroups) {
             const int buf = i % NS;
             double2 *D = Dbuf + buf * PK * kGM;
-            if (i >= NS && !mbar_wait(empty + buf, (i / NS - 1) & 1)) {
+            if (test_stall) return;   // test switch: deliver nothing, no copies issued
+            if (i >= NS && !mbar_wait(empty + buf, (i / NS - 1) & 1, limit)) {
                 atomicExch(status, 1);
                 return;
             }
@@ -529,7 +531,7 @@ __global__ void __launch_bounds__(kTW, 1)
         const int mg = warp & 3, ap = warp >> 2;
         for (uint32_t i = 0; i < ntb; ++i) {
             const int buf = i % NS;
-            if (!mbar_wait(full + buf, (i / NS) & 1)) {
+            if (!mbar_wait(full + buf, (i / NS) & 1, limit)) {
                 if (lane == 0) atomicExch(status, 1);
                 return;
             }
@@ -996,21 +998,24 @@ cudaError_t apply_h_m(const Space &sp, const SpaceTables &tb, const PairOp &op, 
                     return e;
                 if (gw)
                     k_pair_annihilate_gemm_ws<M, 2, true>
-                        <<<gw, kTW, smc2, st>>>(sp, tb, op.hdense, psi, E, ntiles, op.status);
+                        <<<gw, kTW, smc2, st>>>(sp, tb, op.hdense, psi, E, ntiles, op.status,
+                                                                         op.wait_cycles, op.test_stall);
             } else if (smw3 <= (size_t)optin) {
                 if ((e = cudaFuncSetAttribute(k_pair_annihilate_gemm_ws<M, 3, false>,
                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smw3)) != cudaSuccess)
                     return e;
                 if (gw)
                     k_pair_annihilate_gemm_ws<M, 3, false>
-                        <<<gw, kTW, smw3, st>>>(sp, tb, op.hdense, psi, E, ntiles, op.status);
+                        <<<gw, kTW, smw3, st>>>(sp, tb, op.hdense, psi, E, ntiles, op.status,
+                                                                         op.wait_cycles, op.test_stall);
             } else if (smw2 <= (size_t)optin) {
                 if ((e = cudaFuncSetAttribute(k_pair_annihilate_gemm_ws<M, 2, false>,
                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smw2)) != cudaSuccess)
                     return e;
                 if (gw)
                     k_pair_annihilate_gemm_ws<M, 2, false>
-                        <<<gw, kTW, smw2, st>>>(sp, tb, op.hdense, psi, E, ntiles, op.status);
+                        <<<gw, kTW, smw2, st>>>(sp, tb, op.hdense, psi, E, ntiles, op.status,
+                                                                         op.wait_cycles, op.test_stall);
             } else {
                 const size_t smg = G::hbytes + G::dbytes + tab;
                 if ((e = cudaFuncSetAttribute(k_pair_annihilate_gemm<M>,

@@ -28,6 +28,11 @@ struct PairOp {
     // dense form (nullptr unless set): Ht as P x P row-major, for pair matrices with
     // no momentum-block or narrow block structure and P <= kGemmMaxP
     const double2 *hdense;
+    // bounded waits of the warp-specialised dense product: limit in SM cycles
+    // (0: the default, about two seconds) and a test switch that keeps its
+    // gather warps from delivering any tile, so that the waits run out
+    long long wait_cycles;
+    int test_stall;
 };
 constexpr int kGemmMaxP = 78;   // M <= 12: Ht (zero-padded to a multiple of 8 rows) fits shared memory
 

@@ -23,9 +23,12 @@ struct DevPairOp {
     int create_form = 0;
     int *status = nullptr;     // the space's device status word (not owned)
     double2 *hdense = nullptr; // dense form (nullptr unless Ht is general and P <= kGemmMaxP)
+    long long wait_cycles = 0;
+    int test_stall = 0;
     PairOp view() const
     {
-        return PairOp{rowptr, col, val, hdiag, hfull, nnz, hblk, nhblk, create_form, status, hdense};
+        return PairOp{rowptr, col, val, hdiag, hfull, nnz, hblk, nhblk, create_form, status, hdense,
+                      wait_cycles, test_stall};
     }
     BlockOp blocks() const { return BlockOp{prog, prog_bytes}; }
 };
@@ -57,6 +60,8 @@ struct mcpi_space_s {
     bool dense_only = false;         // force the dense pair-matrix kernel
     int kernel_choice = 0;           // 2: skip the momentum-block kernel
     bool no_gemm = false;            // general pair matrices use the CSR kernel (MCPI_OPT_NO_GEMM_KERNEL)
+    long long wait_cycles = 0;       // MCPI_OPT_WAIT_LIMIT_CYCLES
+    int test_stall = 0;              // MCPI_OPT_TEST_STALL_GATHER
     int create_form = 0;            // pair-creation kernel form (MCPI_OPT_CREATE_FORM)
     uint64_t *d_occ = nullptr;       // packed occupations of the space's rows (built by mcpi_set_integrals)
     uint64_t *d_occ2 = nullptr;      // the same for the (N-2)-particle space

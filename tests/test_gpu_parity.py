@@ -295,3 +295,25 @@ def test_apply_h_host_pipeline(orc):
         assert rel(o, refs[k]) <= TOL
     assert sp.apply_h_host([], []) == []
     sp.close()
+
+
+def test_dense_product_wait_timeout_is_reported(orc):
+    # the warp-specialised dense-product kernel's waits are bounded: with its
+    # gather warps held back by the test switch, its product warps give up
+    # after the (shortened) limit, the next synchronisation reports
+    # MCPI_ERR_TIMEOUT, and the space keeps working afterwards
+    N, M = 8, 8
+    C, Ho, Hint = mc.random_problem(N, M, 77)
+    sp = _space(N, M)
+    sp.set_integrals(Ho, Hint)
+    sp.set_option(5, 1000)            # MCPI_OPT_WAIT_LIMIT_KCYCLES: 1e6 cycles
+    sp.set_option(6, 1)               # MCPI_OPT_TEST_STALL_GATHER
+    sp.apply_h(C)
+    with pytest.raises(mc.MCPIError) as err:
+        sp.sync()
+    assert err.value.status == 7      # MCPI_ERR_TIMEOUT
+    sp.set_option(6, 0)
+    out = sp.apply_h(C).cpu().numpy()
+    sp.sync()
+    assert rel(out, orc.apply_h(N, M, C, Ho, Hint, mode=2)) <= TOL
+    sp.close()
