@@ -179,7 +179,10 @@ MCPI_API int mcpi_lanczos(mcpi_space sp, void *d_lvec, int lm, double *h_diag, d
                  int *iters);
 /* Lowest eigenpair of H from niter Lanczos steps started at d_C
  * (groundStateLieb.c:348-471, ground). d_C receives the Ritz vector; *E0 the
- * eigenvalue. Allocates the niter*nc Krylov basis internally. */
+ * eigenvalue. The niter*nc Krylov basis (and mcpi_lanczos's small state and
+ * residual) are workspaces of the space: allocated at the first call that needs
+ * them, reused by later calls, grown when a call needs more, freed by
+ * mcpi_space_destroy. */
 MCPI_API int mcpi_ground(mcpi_space sp, void *d_C, int niter, double *E0, int *iters);
 /* mcpi_ground for spaces whose niter x nc Krylov basis does not fit: plain
  * three-term Lanczos (no reorthogonalisation; same breakdown rule) in two

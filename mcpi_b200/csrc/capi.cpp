@@ -298,6 +298,18 @@ int upload_op(mcpi_space_s *sp, DevPairOp &op, const std::vector<cplx> &Ht, cons
     return MCPI_OK;
 }
 
+// A grow-only device buffer of the space: reused when large enough, else replaced.
+int reserve(void *&ptr, size_t &cap, size_t bytes)
+{
+    if (cap >= bytes && ptr) return MCPI_OK;
+    cudaFree(ptr);
+    ptr = nullptr;
+    cap = 0;
+    CK(cudaMalloc(&ptr, bytes ? bytes : 1));
+    cap = bytes;
+    return MCPI_OK;
+}
+
 int ensure_E(mcpi_space_s *sp)
 {
     if (sp->N < 2 || sp->d_E) return MCPI_OK;
@@ -448,6 +460,9 @@ int mcpi_space_destroy(mcpi_space sp)
     cudaFree(sp->d_status);
     cudaFree(sp->d_occ);
     cudaFree(sp->d_occ2);
+    cudaFree(sp->d_basis);
+    cudaFree(sp->d_lzblk);
+    cudaFree(sp->d_lzr);
     if (sp->s_h2d) cudaStreamSynchronize(sp->s_h2d);
     if (sp->s_d2h) cudaStreamSynchronize(sp->s_d2h);
     for (int b = 0; b < 2; ++b) {
@@ -868,15 +883,14 @@ int mcpi_lanczos(mcpi_space sp, void *d_lvec, int lm, double *h_diag, double *h_
     const int64_t nc = sp->nc;
     const size_t npart = mcpi::lanczos_partial_elems(nc, lm);
     // state block: alpha(lm) coef(lm) partial(npart) | beta(lm) maxbeta | done iters
-    char *blk = nullptr;
     const size_t bytes = sizeof(double2) * (2 * (size_t)lm + npart) + sizeof(double) * (lm + 1) + 2 * sizeof(int);
-    double2 *r = nullptr;
-    CK(cudaMalloc(&blk, bytes));
-    cudaError_t e = cudaMalloc(&r, sizeof(double2) * nc);
-    if (e != cudaSuccess) {
-        cudaFree(blk);
-        return fail(MCPI_ERR_NOMEM, "mcpi_lanczos: %s", cudaGetErrorString(e));
-    }
+    rc = reserve(sp->d_lzblk, sp->lzblk_cap, bytes);
+    if (rc) return rc;
+    rc = reserve(sp->d_lzr, sp->lzr_cap, sizeof(double2) * nc);
+    if (rc) return rc;
+    char *blk = (char *)sp->d_lzblk;
+    double2 *r = (double2 *)sp->d_lzr;
+    cudaError_t e = cudaSuccess;
     mcpi::LanczosState s;
     s.alpha = (double2 *)blk;
     s.coef = s.alpha + lm;
@@ -910,8 +924,6 @@ int mcpi_lanczos(mcpi_space sp, void *d_lvec, int lm, double *h_diag, double *h_
     if (e == cudaSuccess) e = cudaMemcpyAsync(beta.data(), s.beta, sizeof(double) * lm, cudaMemcpyDeviceToHost, sp->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(&it, s.iters, sizeof(int), cudaMemcpyDeviceToHost, sp->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(sp->stream);
-    cudaFree(blk);
-    cudaFree(r);
     if (e != cudaSuccess) return fail(MCPI_ERR_CUDA, "mcpi_lanczos: %s", cudaGetErrorString(e));
     rc = check_status(sp);
     if (rc) return rc;
@@ -935,29 +947,22 @@ int mcpi_ground(mcpi_space sp, void *d_C, int niter, double *E0, int *iters)
     CHECK_ARG(sp && d_C && E0 && niter >= 1, "mcpi_ground: bad arguments");
     DeviceGuard g(sp->device);
     const int64_t nc = sp->nc;
-    double2 *V = nullptr;
-    CK(cudaMalloc(&V, sizeof(double2) * nc * (size_t)niter));
+    int rc0 = reserve(sp->d_basis, sp->basis_cap, sizeof(double2) * nc * (size_t)niter);
+    if (rc0) return rc0;
+    double2 *V = (double2 *)sp->d_basis;
     cudaError_t e = cudaMemcpyAsync(V, d_C, sizeof(double2) * nc, cudaMemcpyDeviceToDevice, sp->stream);
-    if (e != cudaSuccess) {
-        cudaFree(V);
-        return fail(MCPI_ERR_CUDA, "mcpi_ground: %s", cudaGetErrorString(e));
-    }
+    if (e != cudaSuccess) return fail(MCPI_ERR_CUDA, "mcpi_ground: %s", cudaGetErrorString(e));
     std::vector<double> diag(2 * (size_t)niter), off(niter);
     int it = 0;
     int rc = mcpi_lanczos(sp, V, niter, diag.data(), off.data(), &it);
-    if (rc) {
-        cudaFree(V);
-        return rc;
-    }
+    if (rc) return rc;
     // groundStateLieb.c:419-449; a breakdown at the first step keeps alpha_0
     const int n = it > 0 ? it : 1;
     std::vector<double> d(n), ee(n > 1 ? n - 1 : 1), z((size_t)n * n);
     for (int k = 0; k < n; ++k) d[k] = diag[2 * k];
     for (int k = 0; k + 1 < n; ++k) ee[k] = off[k];
-    if (mcpi::tridiag_eig(n, d.data(), ee.data(), z.data()) != 0) {
-        cudaFree(V);
+    if (mcpi::tridiag_eig(n, d.data(), ee.data(), z.data()) != 0)
         return fail(MCPI_ERR_NUMERIC, "tridiagonal QL did not converge");
-    }
     double sentinel = 1e10;
     int jmin = 0;
     for (int k = 0; k < n; ++k)
@@ -973,7 +978,6 @@ int mcpi_ground(mcpi_space sp, void *d_C, int niter, double *E0, int *iters)
     if (e == cudaSuccess) e = mcpi::launch_combine(V, n, nc, dz, (double2 *)d_C, sp->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(sp->stream);
     cudaFree(dz);
-    cudaFree(V);
     if (e != cudaSuccess) return fail(MCPI_ERR_CUDA, "mcpi_ground: %s", cudaGetErrorString(e));
     *E0 = d[jmin];
     if (iters) *iters = it;

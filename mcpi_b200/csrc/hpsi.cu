@@ -893,7 +893,9 @@ __global__ void __launch_bounds__(kTC, 4) k_pair_create_smem(Space sp, SpaceTabl
                                                           double2 *__restrict__ out, uint32_t row0,
                                                           uint32_t row1)
 {
-    create_smem_body<M>(sp, tb, op.hdiag, psi, E, out, blockIdx.x, row0, row1);
+    // blocks run from the top rows down: their E entries (images near the end of
+    // each E row) are the ones kernel 1 wrote last, some still in L2
+    create_smem_body<M>(sp, tb, op.hdiag, psi, E, out, gridDim.x - 1 - blockIdx.x, row0, row1);
 }
 
 // ---------------------------------------------------------------------------

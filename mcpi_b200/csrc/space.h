@@ -63,6 +63,10 @@ struct mcpi_space_s {
     long long wait_cycles = 0;       // MCPI_OPT_WAIT_LIMIT_CYCLES
     int test_stall = 0;              // MCPI_OPT_TEST_STALL_GATHER
     int create_form = 0;            // pair-creation kernel form (MCPI_OPT_CREATE_FORM)
+    // grow-only workspaces kept between calls: Krylov basis of mcpi_ground,
+    // state block and residual of mcpi_lanczos
+    void *d_basis = nullptr, *d_lzblk = nullptr, *d_lzr = nullptr;
+    size_t basis_cap = 0, lzblk_cap = 0, lzr_cap = 0;
     uint64_t *d_occ = nullptr;       // packed occupations of the space's rows (built by mcpi_set_integrals)
     uint64_t *d_occ2 = nullptr;      // the same for the (N-2)-particle space
     int occ_bits = 0;
