@@ -190,8 +190,8 @@ def run_batch(mc, torch, device, iters=120):
         sp = mc.FockSpace(n, m, device=device)
         sp.set_integrals(*mc.lieb_integrals(m, g, L_RING))
         spaces.append((sp, torch.from_numpy(starts[k]).to(sp.torch_device)))
-    sp0, c0 = spaces[0]
-    sp0.ground(c0, iters)                      # warm-up
+    for sp, c in spaces:                       # warm-up: each space allocates its Krylov basis
+        sp.ground(c, iters)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     Es = [sp.ground(c, iters)[0] for sp, c in spaces]

@@ -84,6 +84,10 @@ MCPI_API int mcpi_space_sync(mcpi_space sp);
  * dense-product kernel's gather warps deliver no tile, so its product warps'
  * waits run out (results are invalid while it is set). */
 #define MCPI_OPT_TEST_STALL_GATHER 6
+/* MCPI_OPT_NO_OCC_TABLES (0/1): build no packed occupation tables (the H.psi
+ * kernels then decode every row index; 1 also frees existing tables). Takes
+ * effect at the next mcpi_set_integrals. */
+#define MCPI_OPT_NO_OCC_TABLES 7
 MCPI_API int mcpi_space_set_option(mcpi_space sp, int option, int value);
 MCPI_API int mcpi_space_dims(mcpi_space sp, int *N, int *M, int64_t *nc);
 /* Device memory on the space's device, and a synchronous copy in any direction

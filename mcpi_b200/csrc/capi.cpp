@@ -498,6 +498,17 @@ int mcpi_space_set_option(mcpi_space sp, int option, int value)
         sp->wait_cycles = 1000LL * value;
         sp->fwd.wait_cycles = sp->adj.wait_cycles = sp->wait_cycles;
         return MCPI_OK;
+    case MCPI_OPT_NO_OCC_TABLES:
+        sp->no_occ = value != 0;
+        if (sp->no_occ) {
+            DeviceGuard g(sp->device);
+            cudaStreamSynchronize(sp->stream);
+            cudaFree(sp->d_occ);
+            cudaFree(sp->d_occ2);
+            sp->d_occ = sp->d_occ2 = nullptr;
+            sp->occ_bits = 0;
+        }
+        return MCPI_OK;
     case MCPI_OPT_TEST_STALL_GATHER:
         sp->test_stall = value != 0;
         sp->fwd.test_stall = sp->adj.test_stall = sp->test_stall;
@@ -723,7 +734,7 @@ int mcpi_set_integrals(mcpi_space sp, const double *h_Ho, const double *h_Hint, 
     // skipped, and the kernels decode, when they do not fit 64 bits or memory
     // is short)
     const int bits = mcpi::occ_bits_for(sp->N, sp->M);
-    if (!sp->d_occ && bits && sp->N >= 2 && sp->nc2 > 0) {
+    if (!sp->d_occ && !sp->no_occ && bits && sp->N >= 2 && sp->nc2 > 0) {
         const size_t b1 = sizeof(uint64_t) * (size_t)sp->nc, b2 = sizeof(uint64_t) * (size_t)sp->nc2;
         if (cudaMalloc(&sp->d_occ, b1) == cudaSuccess && cudaMalloc(&sp->d_occ2, b2) == cudaSuccess) {
             const mcpi::SpaceTables t{sp->d_W, sp->d_sq};

@@ -62,6 +62,7 @@ struct mcpi_space_s {
     bool no_gemm = false;            // general pair matrices use the CSR kernel (MCPI_OPT_NO_GEMM_KERNEL)
     long long wait_cycles = 0;       // MCPI_OPT_WAIT_LIMIT_CYCLES
     int test_stall = 0;              // MCPI_OPT_TEST_STALL_GATHER
+    bool no_occ = false;             // MCPI_OPT_NO_OCC_TABLES
     int create_form = 0;            // pair-creation kernel form (MCPI_OPT_CREATE_FORM)
     // grow-only workspaces kept between calls: Krylov basis of mcpi_ground,
     // state block and residual of mcpi_lanczos

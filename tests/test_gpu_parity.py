@@ -317,3 +317,21 @@ def test_dense_product_wait_timeout_is_reported(orc):
     sp.sync()
     assert rel(out, orc.apply_h(N, M, C, Ho, Hint, mode=2)) <= TOL
     sp.close()
+
+
+@pytest.mark.parametrize("N,M,kind", [(9, 8, "lieb"), (7, 9, "random"), (2, 6, "random"), (6, 11, "lieb")])
+def test_occupation_tables_and_decode_agree(orc, N, M, kind):
+    # the H.psi kernels read each row's occupations from the packed tables or,
+    # without them, decode the row index: the results are bit for bit the same
+    C, Ho, Hint = mc.random_problem(N, M, 88)
+    if kind == "lieb":
+        Ho, Hint = mc.lieb_integrals(M, 3.0)
+    sp = _space(N, M)
+    sp.set_integrals(Ho, Hint)
+    with_tables = sp.apply_h(C).cpu().numpy()
+    sp.set_option(7, 1)               # MCPI_OPT_NO_OCC_TABLES
+    sp.set_integrals(Ho, Hint)
+    decoded = sp.apply_h(C).cpu().numpy()
+    assert np.array_equal(with_tables, decoded)
+    assert rel(decoded, orc.apply_h(N, M, C, Ho, Hint, mode=2)) <= TOL
+    sp.close()
