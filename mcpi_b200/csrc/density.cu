@@ -49,7 +49,8 @@ struct Cols {
 // Gathers <m|A_c|x> for the tile's hole configurations into D[c*LD + mt].
 template <int M, int ORDER>
 __device__ __forceinline__ void gather_tile(const Space &sp, const uint32_t *W, const double *sq,
-                                           uint32_t m0, const double2 *__restrict__ x, double2 *D)
+                                           const uint64_t *occ2, int occ_bits, uint32_t m0,
+                                           const double2 *__restrict__ x, double2 *D)
 {
     using C = Cols<M, ORDER>;
     const int mt = threadIdx.x % kTile, cg = threadIdx.x / kTile;
@@ -62,6 +63,10 @@ __device__ __forceinline__ void gather_tile(const Space &sp, const uint32_t *W, 
         return;
     }
     int u[M], Q[M];
+    // decoded here: in this kernel a global load of the packed table per thread
+    // measured slower than the shared-memory decode
+    (void)occ2;
+    (void)occ_bits;
     decode<M>(m, sp.N - ORDER, nh, W, ws, u, Q);
     uint32_t B0[M], B1[M];
     prefix_table<M>(Q, 0, W, ws, B0);
@@ -128,8 +133,8 @@ __global__ void __launch_bounds__(kThreads) k_gram(Space sp, SpaceTables tb,
     const uint32_t ntiles = (nh + kTile - 1) / kTile;
     for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         __syncthreads();
-        gather_tile<M, ORDER>(sp, W, sq, tile * kTile, phi, Dphi);
-        if (!SAME) gather_tile<M, ORDER>(sp, W, sq, tile * kTile, psi, Dpsi);
+        gather_tile<M, ORDER>(sp, W, sq, tb.occ2, tb.occ_bits, tile * kTile, phi, Dphi);
+        if (!SAME) gather_tile<M, ORDER>(sp, W, sq, tb.occ2, tb.occ_bits, tile * kTile, psi, Dpsi);
         __syncthreads();
         if (active) {
 #pragma unroll 4
@@ -153,6 +158,102 @@ __global__ void __launch_bounds__(kThreads) k_gram(Space sp, SpaceTables tb,
 #pragma unroll
             for (int c = 0; c < 4; ++c)
                 if (a0 + r < C::K && b0 + c < C::K) out[(a0 + r) * C::K + (b0 + c)] = acc[r][c];
+    }
+}
+
+// rho1 (and the transition rho1): G[a][b] = sum_h conj(Dphi[a][h]) Dpsi[b][h] over
+// the N-1 space with D[l][h] = sqrt(u_l+1) x[index(h + e_l)]. Only M columns, so
+// the Gram kernel above would keep one 4x4 block per thread busy (9 threads of
+// 256 at M = 10). Here a tile is kTile1 hole configurations, one per thread
+// (one decode each); the product gives every thread one entry (a, b) (a <= b
+// when phi = psi) and one of S interleaved subsets of the tile's
+// configurations; the subsets are summed in a fixed order at the end, so the
+// per-CTA partials (same layout as k_gram's) are deterministic.
+constexpr int kTile1 = 256;
+
+template <int M, bool SAME>
+__global__ void __launch_bounds__(kThreads) k_rho1(Space sp, SpaceTables tb, const double2 *__restrict__ phi,
+                                                   const double2 *__restrict__ psi,
+                                                   double2 *__restrict__ partial)
+{
+    constexpr int LD = kTile1 + 1;                              // row stride (double2)
+    constexpr int NE = SAME ? M * (M + 1) / 2 : M * M;          // entries
+    constexpr int S = NE >= kThreads ? 1 : kThreads / NE;       // configuration subsets
+    static_assert(NE <= kThreads, "one entry per thread");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2 *Dphi = reinterpret_cast<double2 *>(smem_raw);     // M x LD
+    double2 *Dpsi = SAME ? Dphi : Dphi + M * LD;
+    double2 *red = Dphi + (SAME ? 1 : 2) * M * LD;              // kThreads
+    double *sq = reinterpret_cast<double *>(red + kThreads);
+    uint32_t *W = reinterpret_cast<uint32_t *>(sq + sp.wstride);
+    for (int x = threadIdx.x; x < (M - 1) * sp.wstride; x += blockDim.x) W[x] = tb.W[x];
+    for (int x = threadIdx.x; x < sp.wstride; x += blockDim.x) sq[x] = tb.sq[x];
+
+    // this thread's entry and subset
+    const int t = threadIdx.x;
+    const bool active = t < NE * S;
+    const int e = active ? t / S : 0, sub = active ? t % S : 0;
+    int a = 0, b = 0;
+    if (SAME) {
+        int rem = e;   // (a, b), a <= b, in pair order
+        while (rem >= M - a) {
+            rem -= M - a;
+            ++a;
+        }
+        b = a + rem;
+    } else {
+        a = e / M;
+        b = e % M;
+    }
+    double2 acc = make_double2(0.0, 0.0);
+
+    const uint32_t nh = sp.nc1;
+    const uint32_t ntiles = (nh + kTile1 - 1) / kTile1;
+    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        __syncthreads();
+        const uint32_t h = tile * kTile1 + t;
+        if (h < nh) {
+            int u[M], Q[M];
+            decode<M>(h, sp.N - 1, nh, W, sp.wstride, u, Q);
+            uint32_t B0[M], B1[M];
+            prefix_table<M>(Q, 0, W, sp.wstride, B0);
+            prefix_table<M>(Q, 1, W, sp.wstride, B1);
+#pragma unroll
+            for (int l = 0; l < M; ++l) {
+                const uint32_t j = idx_add1(sp.nc, B0, B1, l, M);
+                const double c = sq[u[l] + 1];
+                const double2 x = phi[j];
+                Dphi[l * LD + t] = make_double2(c * x.x, c * x.y);
+                if (!SAME) {
+                    const double2 y = psi[j];
+                    Dpsi[l * LD + t] = make_double2(c * y.x, c * y.y);
+                }
+            }
+        } else {
+#pragma unroll
+            for (int l = 0; l < M; ++l) {
+                Dphi[l * LD + t] = make_double2(0.0, 0.0);
+                if (!SAME) Dpsi[l * LD + t] = make_double2(0.0, 0.0);
+            }
+        }
+        __syncthreads();
+        if (active) {
+#pragma unroll 4
+            for (int i = sub; i < kTile1; i += S) cfma_conj(acc, Dphi[a * LD + i], Dpsi[b * LD + i]);
+        }
+    }
+    __syncthreads();
+    red[t] = acc;
+    __syncthreads();
+    if (active && sub == 0) {
+        double2 g = make_double2(0.0, 0.0);
+        for (int k = 0; k < S; ++k) {
+            g.x += red[e * S + k].x;
+            g.y += red[e * S + k].y;
+        }
+        double2 *out = partial + (size_t)blockIdx.x * M * M;
+        out[a * M + b] = g;
+        if (SAME && a != b) out[b * M + a] = make_double2(g.x, -g.y);
     }
 }
 
@@ -189,6 +290,24 @@ cudaError_t density_m(const Space &sp, const SpaceTables &tb, const double2 *phi
 {
     using C = Cols<M, ORDER>;
     const bool same = (phi == psi);
+    if constexpr (ORDER == 1) {
+        const size_t smem = sizeof(double2) * ((same ? 1 : 2) * (size_t)M * (kTile1 + 1) + kThreads) +
+                            sizeof(double) * sp.wstride + sizeof(uint32_t) * (M - 1) * sp.wstride;
+        const unsigned ntiles = (sp.nc1 + kTile1 - 1) / kTile1;
+        const unsigned gx = ntiles < (unsigned)kGramBlocks ? (ntiles ? ntiles : 1) : kGramBlocks;
+        cudaError_t e;
+        if (same) {
+            e = cudaFuncSetAttribute(k_rho1<M, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+            k_rho1<M, true><<<gx, kThreads, smem, st>>>(sp, tb, phi, psi, partial);
+        } else {
+            e = cudaFuncSetAttribute(k_rho1<M, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+            k_rho1<M, false><<<gx, kThreads, smem, st>>>(sp, tb, phi, psi, partial);
+        }
+        k_gram_finish<M, 1><<<(M * M + 255) / 256, 256, 0, st>>>(partial, gx, out);
+        return cudaGetLastError();
+    }
     const size_t tiles = sizeof(double2) * C::KP * C::LD * (same ? 1 : 2);
     const size_t smem = tiles + sizeof(double) * sp.wstride + sizeof(uint32_t) * (M - 1) * sp.wstride;
     const uint32_t nh = ORDER == 2 ? sp.nc2 : sp.nc1;

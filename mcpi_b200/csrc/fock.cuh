@@ -78,6 +78,27 @@ MCPI_HD void decode(uint32_t idx, int n, uint32_t ncn, const uint32_t *W, int ws
     for (int i = 1; i < M; ++i) v[i] = P[i] - P[i - 1];
 }
 
+// Occupations v and prefix counts P of configuration idx of an n-particle
+// space: from the packed table when there is one, else by decoding the index.
+template <int M>
+MCPI_HD void occupations(const uint64_t *occ, int bits, uint32_t idx, int n, uint32_t ncn,
+                                            const uint32_t *W, int ws, int *v, int *P)
+{
+    if (occ) {
+        const uint64_t w = occ[idx];
+        const uint32_t mask = (1u << bits) - 1u;
+        int run = 0;
+#pragma unroll
+        for (int q = 0; q < M; ++q) {
+            v[q] = (int)((w >> (bits * q)) & mask);
+            run += v[q];
+            P[q] = run;
+        }
+    } else {
+        decode<M>(idx, n, ncn, W, ws, v, P);
+    }
+}
+
 // Prefix sums A[t] = sum_{i<t} W_i(P_i + d), t = 0..M-1 (A[M-1] is the full sum).
 template <int M>
 MCPI_HD void prefix_table(const int *P, int d, const uint32_t *W, int ws, uint32_t *A)

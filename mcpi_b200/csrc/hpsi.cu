@@ -78,27 +78,6 @@ __device__ __forceinline__ void load_tables(const Space &sp, const SpaceTables &
     for (int x = threadIdx.x; x < sp.wstride; x += blockDim.x) sq[x] = tb.sq[x];
 }
 
-// Occupations v and prefix counts P of configuration idx of an n-particle
-// space: from the packed table when there is one, else by decoding the index.
-template <int M>
-__device__ __forceinline__ void occupations(const uint64_t *occ, int bits, uint32_t idx, int n, uint32_t ncn,
-                                            const uint32_t *W, int ws, int *v, int *P)
-{
-    if (occ) {
-        const uint64_t w = occ[idx];
-        const uint32_t mask = (1u << bits) - 1u;
-        int run = 0;
-#pragma unroll
-        for (int q = 0; q < M; ++q) {
-            v[q] = (int)((w >> (bits * q)) & mask);
-            run += v[q];
-            P[q] = run;
-        }
-    } else {
-        decode<M>(idx, n, ncn, W, ws, v, P);
-    }
-}
-
 // ---------------------------------------------------------------------------
 // kernel 1: E[a][m] = sum_b Ht[a][b] c_b(m) psi[index(m + pair b)]
 // ---------------------------------------------------------------------------
