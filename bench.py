@@ -307,12 +307,21 @@ def run_general(mc, torch, device):
         torch.cuda.synchronize()
         ms = a.elapsed_time(b) / reps
         k1, k2 = sp.apply_h_profile(X[0], y, reps=20)
+        dens = {}
+        for name, f in (("rho1_ms", sp.rho1), ("rho2_ms", sp.rho2)):
+            f(X[0])                                   # first call allocates its buffer
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            f(X[0])
+            b.record()
+            b.synchronize()
+            dens[name] = a.elapsed_time(b)
         flops = 8.0 * P * P * nc2
         tf = flops / (k1 * 1e-3) / 1e12
         out[f"n{N}_m{M}"] = {"workload": f"random integrals N={N} M={M} (nc={sp.nc})", "hpsi_ms": ms,
                              "hpsi_per_s": 1e3 / ms, "pair_annihilate_ms": k1, "pair_create_ms": k2,
                              "pair_annihilate_tflops": tf, "pair_annihilate_frac_of_dgemm": tf / peak,
-                             "pair_annihilate_flops": flops}
+                             "pair_annihilate_flops": flops, **dens}
         sp.close()
         del X, y
         torch.cuda.empty_cache()

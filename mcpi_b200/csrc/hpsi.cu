@@ -850,9 +850,10 @@ __device__ __forceinline__ void create_smem_body(const Space &sp, const SpaceTab
                     }
                 const int s = k + rem;
                 const double c = r1[k * kTC + t] * ((s == k) ? sq[vb[k * kTC + t]] : r1[s * kTC + t]);
-                const uint32_t mm = c != 0.0 ? Xr[k * kTC + t] - Yr[s * kTC + t] : 0u;
+                const uint32_t mm = Xr[k * kTC + t] - Yr[s * kTC + t];
                 cc[j] = c;
-                ee[j] = __ldcs(E + (size_t)p * stride + mm);
+                // empty pairs (c = 0: their index is meaningless) load nothing
+                ee[j] = c != 0.0 ? __ldcs(E + (size_t)p * stride + mm) : make_double2(0.0, 0.0);
             }
         }
 #pragma unroll
