@@ -30,7 +30,7 @@ namespace mcpi {
 
 namespace {
 
-constexpr int kT1 = 64;    // threads (= (N-2)-configurations) per block, kernel 1
+constexpr int kT1 = 64;    // threads (= (N-2)-configurations) per block, kernel 1 (compressed-row form)
 constexpr int kCsrStaged = 1024;   // pair-matrix nonzeros staged in shared memory
 constexpr int kT2 = 256;   // threads per block, kernel 2 (register form) and kernel 1 (momentum form)
 constexpr int kTC = 256;   // threads (= rows) per block, kernel 2 (shared-table form)
@@ -172,7 +172,7 @@ __global__ void __launch_bounds__(kT1) k_pair_annihilate(Space sp, SpaceTables t
 //                               the scaling in the product warps), rows b >= P zero
 // ---------------------------------------------------------------------------
 constexpr int kTG = 256;   // threads per block, dense-product form
-constexpr int kGM = 64;    // (N-2)-configurations per tile (8 warps x 8)
+constexpr int kGM = 64;    // (N-2)-configurations per tile (4 MMA row groups of 16)
 
 // m16n8k4: A 16 x 4 (a0 row g, a1 row g + 8; column t), B 4 x 8 (row t, column g),
 // C 16 x 8 (c0, c1 row g, c2, c3 row g + 8; columns 2t, 2t + 1), g = lane / 4, t = lane % 4
@@ -356,7 +356,7 @@ __global__ void __launch_bounds__(kTG, M <= 10 ? 2 : 1)
     using G = GemmShape<M>;
     constexpr int P = G::P, PA = G::PA, PK = G::PK, HS = G::HS;
     constexpr int kParts = kTG / kGM;
-    static_assert(kTG == 256 && kGM == 64, "8 warps x 8 configurations");
+    static_assert(kTG == 256 && kGM == 64, "8 warps: 4 groups of 16 configurations x 2 halves of the pair tiles");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double2 *Hs = reinterpret_cast<double2 *>(smem_raw);          // PA x HS
     double2 *D = Hs + PA * HS;                                    // PK x kGM
