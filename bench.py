@@ -59,6 +59,8 @@ def parse():
     p.add_argument("--no-batch", action="store_true")
     p.add_argument("--no-large", action="store_true")
     p.add_argument("--no-general", action="store_true")
+    p.add_argument("--profile", choices=["batch", "lanczos"], default=None,
+                   help="run only this section (for profiler launch lists), print its timings")
     return p.parse_args()
 
 
@@ -572,8 +574,49 @@ def run_mcpi(args):
         dist.destroy_process_group()
 
 
+def run_profile(args):
+    """One section alone, for ncu: 'batch' = the 64-member sweep (graph capture
+    with the autotuner, then one replay); 'lanczos' = one 150-step ground state
+    of the N=16, M=10 workload after a warm-up solve."""
+    import torch
+
+    import mcpi_b200 as mc
+    if args.profile == "batch":
+        members = batch_members()
+        b = mc.Batch([(n, m) for n, m, _ in members], 120, device=0)
+        for k, (n, m, g) in enumerate(members):
+            b.set_integrals(k, *mc.lieb_integrals(m, g, L_RING))
+            rng = np.random.default_rng(300 + k)
+            C = rng.standard_normal(b.nc[k]) + 1j * rng.standard_normal(b.nc[k])
+            b.set_start(k, C / np.linalg.norm(C))
+        b.run()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        b.run()
+        dt = time.perf_counter() - t0
+        out = {"section": "batch", "seconds": dt, "schedule": b.schedule()[0]}
+        b.close()
+    else:
+        sp = mc.FockSpace(N_PART, M_ORB, device=0)
+        sp.set_integrals(*mc.lieb_integrals(M_ORB, G, L_RING))
+        gen = torch.Generator(device=sp.torch_device)
+        gen.manual_seed(1234)
+        x = torch.randn(sp.nc, dtype=torch.complex128, device=sp.torch_device, generator=gen)
+        x /= torch.linalg.vector_norm(x)
+        sp.ground(x, LANCZOS_ITERS)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        E0, _, it = sp.ground(x, LANCZOS_ITERS)
+        out = {"section": "lanczos", "seconds": time.perf_counter() - t0, "E0": E0, "iterations": it}
+        sp.close()
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
+    if args.profile:
+        run_profile(args)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:
