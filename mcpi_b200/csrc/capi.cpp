@@ -278,6 +278,8 @@ int upload_op(mcpi_space_s *sp, DevPairOp &op, const std::vector<cplx> &Ht, cons
         CK(cudaMalloc(&op.hblk, sizeof(double2) * mom.size()));
         CK(cudaMemcpyAsync(op.hblk, mom.data(), sizeof(double2) * mom.size(), cudaMemcpyHostToDevice, sp->stream));
         op.nhblk = (int)mom.size();
+        op.hblk_h.resize(mom.size());
+        std::memcpy(op.hblk_h.data(), mom.data(), sizeof(double2) * mom.size());
     }
     const std::vector<int> prog = pack_blocks(Ht, P, M);
     if (!prog.empty() && !sp->dense_only) {

@@ -625,18 +625,24 @@ __global__ void __launch_bounds__(kT1b) k_pair_annihilate_blocks(Space sp, Space
 // unrolling: the prefix tables and gathered values stay in registers.
 // hblk holds the blocks' dense values in that order (row-major per block).
 // ---------------------------------------------------------------------------
-template <int M>
+// PARAM: hblk points at a __grid_constant__ kernel parameter; every block value
+// index below is a compile-time constant, so its reads are constant-bank
+// operands. Otherwise hblk is global memory and the values are staged in
+// shared memory.
+template <int M, bool PARAM = false>
 __device__ __forceinline__ void annihilate_momentum_body(const Space &sp, const SpaceTables &tb,
                                                          const double2 *__restrict__ hblk, int nh,
                                                          const double2 *__restrict__ psi,
                                                          double2 *__restrict__ E, uint32_t block)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    double2 *hv = reinterpret_cast<double2 *>(smem_raw);          // nh
-    double *sq = reinterpret_cast<double *>(hv + nh);             // wstride
+    double2 *hs = reinterpret_cast<double2 *>(smem_raw);          // nh (staged form only)
+    double *sq = reinterpret_cast<double *>(hs + (PARAM ? 0 : nh)); // wstride
     uint32_t *W = reinterpret_cast<uint32_t *>(sq + sp.wstride);  // (M-1) x wstride
     load_tables(sp, tb, W, sq);
-    for (int x = threadIdx.x; x < nh; x += blockDim.x) hv[x] = hblk[x];
+    if (!PARAM)
+        for (int x = threadIdx.x; x < nh; x += blockDim.x) hs[x] = hblk[x];
+    const double2 *hv = PARAM ? hblk : hs;
     __syncthreads();
 
     const uint32_t m = block * kT2 + threadIdx.x;
@@ -696,6 +702,32 @@ __global__ void __launch_bounds__(kT2, 3) k_pair_annihilate_momentum(Space sp, S
                                                                   double2 *__restrict__ E)
 {
     annihilate_momentum_body<M>(sp, tb, hblk, nh, psi, E, blockIdx.x);
+}
+
+// Number of momentum-block values for M orbitals (sum over K of block size squared).
+template <int M>
+constexpr int mom_values()
+{
+    int s = 0;
+    for (int K = 0; K <= 2 * M - 2; ++K) {
+        const int qlo = K - (M - 1) > 0 ? K - (M - 1) : 0, n = K / 2 - qlo + 1;
+        s += n * n;
+    }
+    return s;
+}
+
+template <int M>
+struct MomBlocks {
+    double2 v[mom_values<M>()];
+};
+
+template <int M>
+__global__ void __launch_bounds__(kT2, 3) k_pair_annihilate_momentum_p(Space sp, SpaceTables tb,
+                                                                    const __grid_constant__ MomBlocks<M> hp,
+                                                                    const double2 *__restrict__ psi,
+                                                                    double2 *__restrict__ E)
+{
+    annihilate_momentum_body<M, true>(sp, tb, hp.v, mom_values<M>(), psi, E, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -945,9 +977,15 @@ cudaError_t apply_h_m(const Space &sp, const SpaceTables &tb, const PairOp &op, 
     constexpr int P = M * (M + 1) / 2;
     const size_t tab = sizeof(double) * sp.wstride + sizeof(uint32_t) * (M - 1) * sp.wstride;
     if (sp.N >= 2 && (stages & 1) && op.hblk) {
-        const size_t smm = sizeof(double2) * op.nhblk + tab;
         const unsigned g1 = (sp.nc2 + kT2 - 1) / kT2;
-        k_pair_annihilate_momentum<M><<<g1, kT2, smm, st>>>(sp, tb, op.hblk, op.nhblk, psi, E);
+        if (op.hblk_host && op.nhblk == mom_values<M>()) {
+            MomBlocks<M> hp;
+            for (int x = 0; x < mom_values<M>(); ++x) hp.v[x] = op.hblk_host[x];
+            k_pair_annihilate_momentum_p<M><<<g1, kT2, tab, st>>>(sp, tb, hp, psi, E);
+        } else {
+            const size_t smm = sizeof(double2) * op.nhblk + tab;
+            k_pair_annihilate_momentum<M><<<g1, kT2, smm, st>>>(sp, tb, op.hblk, op.nhblk, psi, E);
+        }
     } else if (sp.N >= 2 && (stages & 1) && bo.prog) {
         const size_t smb = ((bo.bytes + 15) & ~15) + (2 * sizeof(double) + 2 * sizeof(uint32_t)) * M * kT1b + tab;
         if (smb > 48 * 1024) {

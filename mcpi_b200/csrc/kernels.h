@@ -33,6 +33,10 @@ struct PairOp {
     // gather warps from delivering any tile, so that the waits run out
     long long wait_cycles;
     int test_stall;
+    // host copy of hblk (nhblk values) or null: the momentum kernel then takes
+    // the block values as a kernel parameter (constant bank) instead of
+    // staging them in shared memory
+    const double2 *hblk_host;
 };
 constexpr int kGemmMaxP = 78;   // M <= 12: Ht (zero-padded to a multiple of 8 rows) fits shared memory
 

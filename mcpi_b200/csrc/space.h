@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
 #include "../../include/mcpi_b200.h"
 #include "kernels.h"
 
@@ -20,6 +22,7 @@ struct DevPairOp {
     int prog_bytes = 0;
     double2 *hblk = nullptr;   // momentum-block form (nullptr when Ht couples different q+l)
     int nhblk = 0;
+    std::vector<double2> hblk_h;   // host copy of hblk
     int create_form = 0;
     int *status = nullptr;     // the space's device status word (not owned)
     double2 *hdense = nullptr; // dense form (nullptr unless Ht is general and P <= kGemmMaxP)
@@ -28,7 +31,7 @@ struct DevPairOp {
     PairOp view() const
     {
         return PairOp{rowptr, col, val, hdiag, hfull, nnz, hblk, nhblk, create_form, status, hdense,
-                      wait_cycles, test_stall};
+                      wait_cycles, test_stall, hblk_h.empty() ? nullptr : hblk_h.data()};
     }
     BlockOp blocks() const { return BlockOp{prog, prog_bytes}; }
 };
