@@ -119,10 +119,14 @@ __global__ void __launch_bounds__(kThreads) k_gram(Space sp, SpaceTables tb,
         if (!SAME) Dpsi[C::K * C::LD + x] = make_double2(0.0, 0.0);
     }
 
-    // output block of this thread
+    // output block of this thread: rows aa + r*NB and columns bb + c*NB
+    // (r, c < 4). Interleaved rather than four consecutive rows: the row
+    // stride LD = 33 double2 puts row x in 16-byte bank slot (x + t) mod 8, so
+    // a warp's ~14 distinct bb land on all eight slots (2 wavefronts per load)
+    // where the consecutive form (rows 4*bb + c) hit only two (7 wavefronts).
     const int blk = blockIdx.y * kThreads + threadIdx.x;
     const bool active = blk < C::NB * C::NB;
-    const int a0 = active ? (blk / C::NB) * 4 : 0, b0 = active ? (blk % C::NB) * 4 : 0;
+    const int aa = active ? blk / C::NB : 0, bb = active ? blk % C::NB : 0;
     double2 acc[4][4];
 #pragma unroll
     for (int r = 0; r < 4; ++r)
@@ -141,9 +145,9 @@ __global__ void __launch_bounds__(kThreads) k_gram(Space sp, SpaceTables tb,
             for (int t = 0; t < kTile; ++t) {
                 double2 pa[4], pb[4];
 #pragma unroll
-                for (int r = 0; r < 4; ++r) pa[r] = Dphi[(a0 + r) * C::LD + t];
+                for (int r = 0; r < 4; ++r) pa[r] = Dphi[(aa + r * C::NB) * C::LD + t];
 #pragma unroll
-                for (int c = 0; c < 4; ++c) pb[c] = Dpsi[(b0 + c) * C::LD + t];
+                for (int c = 0; c < 4; ++c) pb[c] = Dpsi[(bb + c * C::NB) * C::LD + t];
 #pragma unroll
                 for (int r = 0; r < 4; ++r)
 #pragma unroll
@@ -157,7 +161,8 @@ __global__ void __launch_bounds__(kThreads) k_gram(Space sp, SpaceTables tb,
         for (int r = 0; r < 4; ++r)
 #pragma unroll
             for (int c = 0; c < 4; ++c)
-                if (a0 + r < C::K && b0 + c < C::K) out[(a0 + r) * C::K + (b0 + c)] = acc[r][c];
+                if (aa + r * C::NB < C::K && bb + c * C::NB < C::K)
+                    out[(aa + r * C::NB) * C::K + (bb + c * C::NB)] = acc[r][c];
     }
 }
 
