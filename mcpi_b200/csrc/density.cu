@@ -124,9 +124,25 @@ __global__ void __launch_bounds__(kThreads) k_gram(Space sp, SpaceTables tb,
     // stride LD = 33 double2 puts row x in 16-byte bank slot (x + t) mod 8, so
     // a warp's ~14 distinct bb land on all eight slots (2 wavefronts per load)
     // where the consecutive form (rows 4*bb + c) hit only two (7 wavefronts).
+    // With phi = psi the Gram matrix is Hermitian: only the blocks with
+    // aa <= bb are reduced (NB(NB+1)/2 of NB^2) and k_gram_finish takes the
+    // others as conjugates of their mirror entries.
     const int blk = blockIdx.y * kThreads + threadIdx.x;
-    const bool active = blk < C::NB * C::NB;
-    const int aa = active ? blk / C::NB : 0, bb = active ? blk % C::NB : 0;
+    const bool active = blk < (SAME ? C::NB * (C::NB + 1) / 2 : C::NB * C::NB);
+    int aa = 0, bb = 0;
+    if (active) {
+        if (SAME) {
+            int rem = blk;
+            while (rem >= C::NB - aa) {
+                rem -= C::NB - aa;
+                ++aa;
+            }
+            bb = aa + rem;
+        } else {
+            aa = blk / C::NB;
+            bb = blk % C::NB;
+        }
+    }
     double2 acc[4][4];
 #pragma unroll
     for (int r = 0; r < 4; ++r)
@@ -263,7 +279,9 @@ __global__ void __launch_bounds__(kThreads) k_rho1(Space sp, SpaceTables tb, con
 }
 
 // Sums the per-CTA partials in block order and writes the reference layout.
-template <int M, int ORDER>
+// HERM: the partials hold only the blocks of k_gram<.., SAME = true> (entry
+// (a, b) with a mod NB <= b mod NB); the rest is conj of the entry (b, a).
+template <int M, int ORDER, bool HERM = false>
 __global__ void k_gram_finish(const double2 *__restrict__ partial, int nblocks,
                               double2 *__restrict__ out)
 {
@@ -280,12 +298,15 @@ __global__ void k_gram_finish(const double2 *__restrict__ partial, int nblocks,
         a = k <= s ? pair_index(k, s, M) : pair_index(s, k, M);
         b = q <= l ? pair_index(q, l, M) : pair_index(l, q, M);
     }
+    const bool mirror = HERM && (a % C::NB) > (b % C::NB);
+    const int e = mirror ? b * C::K + a : a * C::K + b;
     double2 acc = make_double2(0.0, 0.0);
     for (int blk = 0; blk < nblocks; ++blk) {
-        const double2 p = partial[(size_t)blk * C::K * C::K + a * C::K + b];
+        const double2 p = partial[(size_t)blk * C::K * C::K + e];
         acc.x += p.x;
         acc.y += p.y;
     }
+    if (mirror) acc.y = -acc.y;
     out[x] = acc;
 }
 
@@ -318,7 +339,8 @@ cudaError_t density_m(const Space &sp, const SpaceTables &tb, const double2 *phi
     const uint32_t nh = ORDER == 2 ? sp.nc2 : sp.nc1;
     const unsigned ntiles = (nh + kTile - 1) / kTile;
     const unsigned gx = ntiles < (unsigned)kGramBlocks ? (ntiles ? ntiles : 1) : kGramBlocks;
-    const unsigned gy = (C::NB * C::NB + kThreads - 1) / kThreads;
+    const unsigned nblk = same ? C::NB * (C::NB + 1) / 2 : C::NB * C::NB;
+    const unsigned gy = (nblk + kThreads - 1) / kThreads;
     dim3 grid(gx, gy);
     cudaError_t e;
     if (same) {
@@ -331,7 +353,10 @@ cudaError_t density_m(const Space &sp, const SpaceTables &tb, const double2 *phi
         k_gram<M, ORDER, false><<<grid, kThreads, smem, st>>>(sp, tb, phi, psi, partial);
     }
     const int nout = ORDER == 1 ? M * M : M * M * M * M;
-    k_gram_finish<M, ORDER><<<(nout + 255) / 256, 256, 0, st>>>(partial, gx, out);
+    if (same)
+        k_gram_finish<M, ORDER, true><<<(nout + 255) / 256, 256, 0, st>>>(partial, gx, out);
+    else
+        k_gram_finish<M, ORDER, false><<<(nout + 255) / 256, 256, 0, st>>>(partial, gx, out);
     return cudaGetLastError();
 }
 
