@@ -59,7 +59,7 @@ def parse():
     p.add_argument("--no-batch", action="store_true")
     p.add_argument("--no-large", action="store_true")
     p.add_argument("--no-general", action="store_true")
-    p.add_argument("--profile", choices=["batch", "lanczos"], default=None,
+    p.add_argument("--profile", choices=["batch", "lanczos", "density"], default=None,
                    help="run only this section (for profiler launch lists), print its timings")
     return p.parse_args()
 
@@ -577,7 +577,9 @@ def run_mcpi(args):
 def run_profile(args):
     """One section alone, for ncu: 'batch' = the 64-member sweep (graph capture
     with the autotuner, then one replay); 'lanczos' = one 150-step ground state
-    of the N=16, M=10 workload after a warm-up solve."""
+    of the N=16, M=10 workload after a warm-up solve; 'density' = rho1, rho2
+    and the transition rho2 of seeded N=16, M=10 states (--steps calls each
+    after --warmup, CUDA events)."""
     import torch
 
     import mcpi_b200 as mc
@@ -596,6 +598,29 @@ def run_profile(args):
         dt = time.perf_counter() - t0
         out = {"section": "batch", "seconds": dt, "schedule": b.schedule()[0]}
         b.close()
+    elif args.profile == "density":
+        sp = mc.FockSpace(N_PART, M_ORB, device=0)
+        sp.set_integrals(*mc.lieb_integrals(M_ORB, G, L_RING))
+        gen = torch.Generator(device=sp.torch_device)
+        gen.manual_seed(1234)
+        x, y = (torch.randn(sp.nc, dtype=torch.complex128, device=sp.torch_device, generator=gen)
+                for _ in range(2))
+        x /= torch.linalg.vector_norm(x)
+        y /= torch.linalg.vector_norm(y)
+        out = {"section": "density", "workload": f"Lieb-Liniger N={N_PART} M={M_ORB} (nc={sp.nc})"}
+        for name, f in (("rho1", lambda: sp.rho1(x)), ("rho2", lambda: sp.rho2(x)),
+                        ("trans_rho2", lambda: sp.trans_rho2(y, x))):
+            for _ in range(args.warmup):
+                f()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            a.record()
+            for _ in range(args.steps):
+                f()
+            b.record()
+            torch.cuda.synchronize()
+            out[name + "_ms"] = a.elapsed_time(b) / args.steps
+        sp.close()
     else:
         sp = mc.FockSpace(N_PART, M_ORB, device=0)
         sp.set_integrals(*mc.lieb_integrals(M_ORB, G, L_RING))
