@@ -9,8 +9,9 @@
 //     rho1[k][l]        = sum_{m in N-1}  conj(<m|a_k|phi>)      <m|a_l|psi>
 //     rho2[(k,s),(q,l)] = sum_{m in N-2}  conj(<m|a_k a_s|phi>)  <m|a_q a_l|psi>
 // with phi = psi for rho1/rho2 and phi != psi for the transition densities
-// <phi|a+_k a_l|psi>, <phi|a+_k a+_s a_q a_l|psi> (no symmetry fill is used,
-// so every entry is reduced and the result is valid for phi != psi). One pass
+// <phi|a+_k a_l|psi>, <phi|a+_k a+_s a_q a_l|psi> (for phi != psi every entry
+// is reduced; for one state only the Hermitian half of the Gram matrix is
+// reduced and the rest is its conjugate transpose). One pass
 // over the hole space: a CTA gathers a tile of 32 hole configurations x K
 // columns (K = M or P = M(M+1)/2) of <m|A|.> into shared memory, then each
 // thread accumulates a 4x4 block of the K x K Gram matrix in registers across
