@@ -155,7 +155,10 @@ MCPI_API int mcpi_apply_h_profile(mcpi_space sp, const void *d_C, void *d_out, i
  * the P * NC(N-2,M) intermediate exceed the array (at M = 10: N <= 10).
  * Calls share the array: calls that overlap on the GPU race. The first call
  * on a device looks up the array's device address; make it before any stream
- * capture begins. */
+ * capture begins. Not capturable: a call on a capturing stream (or on the
+ * legacy stream while another stream captures) returns MCPI_ERR_ARG with
+ * nothing enqueued. Each call folds the integrals on the calling thread's
+ * stack, about 58 KB at M = 10. */
 MCPI_API int mcpi_apply_h_static(int N, int M, const double *h_Ho, const double *h_Hint, int variant,
                                  const void *d_C, void *d_out, void *stream);
 /* out = H^dagger C (adjoint of the operator above; equal to H C when Ho is

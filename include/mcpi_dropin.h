@@ -12,7 +12,7 @@
  *
  * include/dropin/ holds replacement configurationsMap.h, hamiltonianMatrix.h,
  * onebodyMatrix.h, twobodyMatrix.h and mkl.h that include this header, so the
- * reference drivers compile unmodified against it (see INTEGRATION.md).
+ * reference drivers compile unmodified against it.
  */
 #ifndef MCPI_DROPIN_H
 #define MCPI_DROPIN_H

@@ -31,6 +31,15 @@ LIB_PATH = os.path.join(HERE, "libmcpi_b200.so")
 VARIANT_MAPS = 0   # applyHconf_X / _XX / _omp and the reference CUDA kernel
 VARIANT_HASH = 1   # applyHconf (plain): Rule 9 summed over every ordering
 
+# space options (mcpi_space_set_option; meanings in include/mcpi_b200.h)
+OPT_DENSE_PAIR_KERNEL = 1
+OPT_NO_MOMENTUM_KERNEL = 2
+OPT_CREATE_FORM = 3
+OPT_NO_GEMM_KERNEL = 4
+OPT_WAIT_LIMIT_KCYCLES = 5
+OPT_TEST_STALL_GATHER = 6
+OPT_NO_OCC_TABLES = 7
+
 
 class MCPIError(RuntimeError):
     """A status other than MCPI_OK returned by the C ABI."""

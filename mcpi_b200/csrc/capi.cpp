@@ -14,6 +14,7 @@
 
 #include "fock.cuh"
 #include "kernels.h"
+#include "pairfold.h"
 #include "space.h"
 
 namespace mcpi {
@@ -104,63 +105,13 @@ void free_op(DevPairOp &o)
     o = DevPairOp{};
 }
 
-// Pair matrix Ht[a][b] (a = (k<=s) creation pair, b = (q<=l) annihilation
-// pair) such that  sum_ab Ht[a][b] a+_k a+_s a_q a_l  equals the reference's
-// two-body sum rule by rule (hamiltonianMatrix.h:976-1418; each rule's factor
-// 1, 2 or 4 times the outer 1/2, on the Hint entry that rule reads), plus the
-// off-diagonal one-body part folded in as a+_k a_l = (N-1)^-1 sum_s a+_k a+_s a_s a_l.
+// Pair matrix Ht of the two-body sum plus the folded off-diagonal one-body
+// part (pairfold.h: rule by rule as hamiltonianMatrix.h:976-1418 reads Hint).
 std::vector<cplx> build_pair_matrix(int N, int M, const cplx *Ho, const cplx *Hint, int variant)
 {
     const int P = M * (M + 1) / 2;
-    const size_t M2 = (size_t)M * M, M3 = M2 * M;
-    std::vector<cplx> Ht((size_t)P * P, cplx(0.0, 0.0));
-    auto H = [&](int k, int s, int q, int l) { return Hint[k + s * M + q * M2 + l * M3]; };
-    auto pr = [&](int a, int b) { return a <= b ? mcpi::pair_index(a, b, M) : mcpi::pair_index(b, a, M); };
-    auto at = [&](int a, int b) -> cplx & { return Ht[(size_t)a * P + b]; };
-    if (N >= 2) {
-        for (int k = 0; k < M; ++k) at(pr(k, k), pr(k, k)) += 0.5 * H(k, k, k, k);           // R1
-        for (int k = 0; k < M; ++k)                                                           // R2
-            for (int s = k + 1; s < M; ++s) at(pr(k, s), pr(k, s)) += 2.0 * H(k, s, k, s);
-        for (int k = 0; k < M; ++k)                                                           // R3
-            for (int q = 0; q < M; ++q)
-                if (q != k) at(pr(k, k), pr(q, q)) += 0.5 * H(k, k, q, q);
-        for (int k = 0; k < M; ++k)                                                           // R4
-            for (int l = 0; l < M; ++l)
-                if (l != k) at(pr(k, k), pr(k, l)) += H(k, k, k, l);
-        for (int k = 0; k < M; ++k)                                                           // R5
-            for (int s = 0; s < M; ++s)
-                if (s != k) at(pr(k, s), pr(s, s)) += H(k, s, s, s);
-        for (int k = 0; k < M; ++k)                                                           // R6
-            for (int q = 0; q < M; ++q)
-                for (int l = q + 1; l < M; ++l)
-                    if (q != k && l != k) at(pr(k, k), pr(q, l)) += H(k, k, q, l);
-        for (int k = 0; k < M; ++k)                                                           // R7
-            for (int s = k + 1; s < M; ++s)
-                for (int q = 0; q < M; ++q)
-                    if (q != k && q != s) at(pr(k, s), pr(q, q)) += H(k, s, q, q);
-        for (int s = 0; s < M; ++s)                                                           // R8
-            for (int k = 0; k < M; ++k)
-                for (int l = 0; l < M; ++l)
-                    if (k != s && l != k && l != s) at(pr(k, s), pr(s, l)) += 2.0 * H(k, s, s, l);
-        for (int k = 0; k < M; ++k)                                                           // R9
-            for (int s = k + 1; s < M; ++s)
-                for (int q = 0; q < M; ++q)
-                    for (int l = q + 1; l < M; ++l) {
-                        if (q == k || q == s || l == k || l == s) continue;
-                        if (variant == MCPI_VARIANT_HASH)
-                            at(pr(k, s), pr(q, l)) +=
-                                0.5 * (H(k, s, q, l) + H(s, k, q, l) + H(k, s, l, q) + H(s, k, l, q));
-                        else
-                            at(pr(k, s), pr(q, l)) += 2.0 * H(k, s, q, l);
-                    }
-        // off-diagonal one-body, folded
-        const double f = 1.0 / (N - 1);
-        for (int k = 0; k < M; ++k)
-            for (int l = 0; l < M; ++l) {
-                if (k == l || Ho[k * M + l] == cplx(0.0, 0.0)) continue;
-                for (int s = 0; s < M; ++s) at(pr(k, s), pr(s, l)) += f * Ho[k * M + l];
-            }
-    }
+    std::vector<cplx> Ht((size_t)P * P);
+    mcpi::fold_pair_matrix(N, M, Ho, Hint, variant == MCPI_VARIANT_HASH, Ht.data());
     return Ht;
 }
 
@@ -447,6 +398,48 @@ int mcpi_space_create(int N, int M, int device, mcpi_space *out)
     return MCPI_OK;
 }
 
+// Releases the host-buffer pipeline of mcpi_apply_h_host (whatever of it exists).
+static void free_host_pipe(mcpi_space sp)
+{
+    if (sp->s_h2d) cudaStreamSynchronize(sp->s_h2d);
+    if (sp->s_d2h) cudaStreamSynchronize(sp->s_d2h);
+    for (int b = 0; b < 2; ++b) {
+        cudaFree(sp->d_hin[b]);
+        cudaFree(sp->d_hout[b]);
+        if (sp->ev_in[b]) cudaEventDestroy(sp->ev_in[b]);
+        if (sp->ev_comp[b]) cudaEventDestroy(sp->ev_comp[b]);
+        if (sp->ev_out[b]) cudaEventDestroy(sp->ev_out[b]);
+        sp->d_hin[b] = sp->d_hout[b] = nullptr;
+        sp->ev_in[b] = sp->ev_comp[b] = sp->ev_out[b] = nullptr;
+    }
+    if (sp->s_h2d) cudaStreamDestroy(sp->s_h2d);
+    if (sp->s_d2h) cudaStreamDestroy(sp->s_d2h);
+    sp->s_h2d = sp->s_d2h = nullptr;
+    sp->host_pipe_ready = false;
+}
+
+// Creates the pipeline: two streams, two input and two output buffers, and
+// their events. On any failure everything created so far is released, so a
+// later call starts again from nothing.
+static cudaError_t make_host_pipe(mcpi_space sp, size_t bytes)
+{
+    cudaError_t e = cudaStreamCreateWithFlags(&sp->s_h2d, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&sp->s_d2h, cudaStreamNonBlocking);
+    for (int b = 0; b < 2 && e == cudaSuccess; ++b) {
+        e = cudaMalloc(&sp->d_hin[b], bytes);
+        if (e == cudaSuccess) e = cudaMalloc(&sp->d_hout[b], bytes);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sp->ev_in[b], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sp->ev_comp[b], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sp->ev_out[b], cudaEventDisableTiming);
+    }
+    if (e != cudaSuccess) {
+        free_host_pipe(sp);
+        return e;
+    }
+    sp->host_pipe_ready = true;
+    return cudaSuccess;
+}
+
 int mcpi_space_destroy(mcpi_space sp)
 {
     if (!sp) return MCPI_OK;
@@ -465,17 +458,7 @@ int mcpi_space_destroy(mcpi_space sp)
     cudaFree(sp->d_basis);
     cudaFree(sp->d_lzblk);
     cudaFree(sp->d_lzr);
-    if (sp->s_h2d) cudaStreamSynchronize(sp->s_h2d);
-    if (sp->s_d2h) cudaStreamSynchronize(sp->s_d2h);
-    for (int b = 0; b < 2; ++b) {
-        cudaFree(sp->d_hin[b]);
-        cudaFree(sp->d_hout[b]);
-        if (sp->ev_in[b]) cudaEventDestroy(sp->ev_in[b]);
-        if (sp->ev_comp[b]) cudaEventDestroy(sp->ev_comp[b]);
-        if (sp->ev_out[b]) cudaEventDestroy(sp->ev_out[b]);
-    }
-    if (sp->s_h2d) cudaStreamDestroy(sp->s_h2d);
-    if (sp->s_d2h) cudaStreamDestroy(sp->s_d2h);
+    free_host_pipe(sp);
     if (sp->own) cudaStreamDestroy(sp->own);
     delete sp;
     return MCPI_OK;
@@ -768,17 +751,7 @@ int mcpi_apply_h_host(mcpi_space sp, int count, const void *const *h_C, void *co
     int rc = ensure_E(sp);
     if (rc) return rc;
     const size_t bytes = sizeof(double2) * (size_t)sp->nc;
-    if (!sp->s_h2d) {
-        CK(cudaStreamCreateWithFlags(&sp->s_h2d, cudaStreamNonBlocking));
-        CK(cudaStreamCreateWithFlags(&sp->s_d2h, cudaStreamNonBlocking));
-        for (int b = 0; b < 2; ++b) {
-            CK(cudaMalloc(&sp->d_hin[b], bytes));
-            CK(cudaMalloc(&sp->d_hout[b], bytes));
-            CK(cudaEventCreateWithFlags(&sp->ev_in[b], cudaEventDisableTiming));
-            CK(cudaEventCreateWithFlags(&sp->ev_comp[b], cudaEventDisableTiming));
-            CK(cudaEventCreateWithFlags(&sp->ev_out[b], cudaEventDisableTiming));
-        }
-    }
+    if (!sp->host_pipe_ready) CK(make_host_pipe(sp, bytes));
     // buffer pair b = k & 1: its input is free once H.psi of state k-2 has run,
     // its output once the copy out of state k-2 has finished
     for (int k = 0; k < count; ++k) {

@@ -27,6 +27,18 @@
 // g_scratch with cudaGetSymbolAddress (host code cannot use the symbol itself
 // as a device pointer) while that device is current, and caches it; make that
 // first call before any stream capture begins.
+//
+// Not for stream capture: each call copies its freshly folded tables from
+// buffers on the calling thread's stack with pageable cudaMemcpyAsync, which a
+// captured graph could not replay (the buffers are gone by then). A call on a
+// stream that is capturing -- or on the legacy default stream while another
+// stream captures -- returns MCPI_ERR_ARG before it enqueues anything, so the
+// caller's capture stays intact.
+//
+// Host stack: the folded pair matrix (P*P complex, compacted in place into
+// the nonzero values), its column indices and the binomial tables take about
+// 58 KB of the calling thread's stack at M = 10; threads with small stacks
+// (some worker pools, musl's 128 KB default) must leave room for that.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -37,6 +49,7 @@
 #include "../../include/mcpi_b200.h"
 #include "fock.cuh"
 #include "kernels.h"
+#include "pairfold.h"
 
 namespace {
 
@@ -64,55 +77,6 @@ int64_t binom64(int n, int k)   // exact for the small arguments admitted here
     return (int64_t)r;
 }
 
-// Pair matrix of the two-body sum as the reference folds it (each rule's
-// factor times 1/2 on the Hint entry it reads; variant MCPI_VARIANT_HASH sums
-// Rule 9 over all orderings), plus the off-diagonal one-body terms folded in
-// as a+_k a_l = (N-1)^-1 sum_s a+_k a+_s a_s a_l. Writes P*P entries.
-void fold_pairs(int N, int M, const cplx *Ho, const cplx *Hint, int variant, cplx *Ht)
-{
-    const int P = M * (M + 1) / 2;
-    for (int x = 0; x < P * P; ++x) Ht[x] = 0.0;
-    if (N < 2) return;
-    const int M2 = M * M, M3 = M2 * M;
-    auto H = [&](int k, int s, int q, int l) { return Hint[k + s * M + q * M2 + l * M3]; };
-    auto pr = [&](int a, int b) { return a <= b ? mcpi::pair_index(a, b, M) : mcpi::pair_index(b, a, M); };
-    auto at = [&](int a, int b) -> cplx & { return Ht[a * P + b]; };
-    for (int k = 0; k < M; ++k) {
-        at(pr(k, k), pr(k, k)) += 0.5 * H(k, k, k, k);
-        for (int s = 0; s < M; ++s) {
-            if (s == k) continue;
-            if (s > k) at(pr(k, s), pr(k, s)) += 2.0 * H(k, s, k, s);
-            at(pr(k, k), pr(s, s)) += 0.5 * H(k, k, s, s);
-            at(pr(k, k), pr(k, s)) += H(k, k, k, s);
-            at(pr(k, s), pr(s, s)) += H(k, s, s, s);
-        }
-        for (int q = 0; q < M; ++q)
-            for (int l = q + 1; l < M; ++l)
-                if (q != k && l != k) at(pr(k, k), pr(q, l)) += H(k, k, q, l);
-    }
-    for (int k = 0; k < M; ++k)
-        for (int s = k + 1; s < M; ++s)
-            for (int q = 0; q < M; ++q) {
-                if (q == k || q == s) continue;
-                at(pr(k, s), pr(q, q)) += H(k, s, q, q);
-                for (int l = q + 1; l < M; ++l) {
-                    if (l == k || l == s) continue;
-                    at(pr(k, s), pr(q, l)) += variant == MCPI_VARIANT_HASH
-                                                  ? 0.5 * (H(k, s, q, l) + H(s, k, q, l) + H(k, s, l, q) + H(s, k, l, q))
-                                                  : 2.0 * H(k, s, q, l);
-                }
-            }
-    for (int s = 0; s < M; ++s)
-        for (int k = 0; k < M; ++k)
-            for (int l = 0; l < M; ++l)
-                if (k != s && l != k && l != s) at(pr(k, s), pr(s, l)) += 2.0 * H(k, s, s, l);
-    const double f = 1.0 / (N - 1);
-    for (int k = 0; k < M; ++k)
-        for (int l = 0; l < M; ++l)
-            if (k != l && Ho[k * M + l] != cplx(0.0, 0.0))
-                for (int s = 0; s < M; ++s) at(pr(k, s), pr(s, l)) += f * Ho[k * M + l];
-}
-
 }  // namespace
 
 extern "C" MCPI_API int mcpi_apply_h_static(int N, int M, const double *h_Ho, const double *h_Hint,
@@ -137,6 +101,14 @@ extern "C" MCPI_API int mcpi_apply_h_static(int N, int M, const double *h_Ho, co
     const size_t need = oE + sizeof(double2) * (size_t)P * (size_t)nc2;
     if (need > kScratchBytes || nc >= ((int64_t)1 << 31)) return MCPI_ERR_RANGE;
 
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    {
+        // refuse capture before touching anything else (see the file comment);
+        // an error from the query itself (the legacy stream while another
+        // stream captures globally) counts as capturing
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return MCPI_ERR_ARG;
+    }
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return MCPI_ERR_CUDA;
     unsigned char *base;
@@ -150,31 +122,35 @@ extern "C" MCPI_API int mcpi_apply_h_static(int N, int M, const double *h_Ho, co
         base = static_cast<unsigned char *>(g_scratch_ptr[dev]);
     }
 
-    // host-side tables, on the stack
+    // host-side tables, on the stack (about 58 KB at M = 10)
     uint32_t W[(kMaxStaticM - 1) * kMaxStaticWs];
     double sq[kMaxStaticWs];
     int rowptr[kMaxStaticP + 1];
     uint16_t col[kMaxStaticP * kMaxStaticP];
-    cplx val[kMaxStaticP * kMaxStaticP], Ht[kMaxStaticP * kMaxStaticP], hd[kMaxStaticM];
+    cplx Ht[kMaxStaticP * kMaxStaticP], hd[kMaxStaticM];
     for (int i = 0; i + 1 < M; ++i)
         for (int p = 0; p < ws; ++p) W[i * ws + p] = (uint32_t)binom64(p + i, i + 1);
     for (int n = 0; n < ws; ++n) sq[n] = std::sqrt((double)n);
     const cplx *Ho = reinterpret_cast<const cplx *>(h_Ho);
     const cplx *Hint = reinterpret_cast<const cplx *>(h_Hint);
-    fold_pairs(N, M, Ho, Hint, variant, Ht);
+    mcpi::fold_pair_matrix(N, M, Ho, Hint, variant == MCPI_VARIANT_HASH, Ht);
+    // compressed rows, compacted in place: entry nnz is written only after
+    // entry a * P + b >= nnz has been read
+    cplx *val = Ht;
     int nnz = 0;
     for (int a = 0; a < P; ++a) {
         rowptr[a] = nnz;
-        for (int b = 0; b < P; ++b)
-            if (Ht[a * P + b] != cplx(0.0, 0.0)) {
+        for (int b = 0; b < P; ++b) {
+            const cplx h = Ht[a * P + b];
+            if (h != cplx(0.0, 0.0)) {
                 col[nnz] = (uint16_t)b;
-                val[nnz++] = Ht[a * P + b];
+                val[nnz++] = h;
             }
+        }
     }
     rowptr[P] = nnz;
     for (int k = 0; k < M; ++k) hd[k] = Ho[k * M + k];
 
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
     cudaError_t e = cudaSuccess;
     auto put = [&](size_t off, const void *src, size_t bytes) {
         if (e == cudaSuccess && bytes) e = cudaMemcpyAsync(base + off, src, bytes, cudaMemcpyHostToDevice, st);

@@ -51,6 +51,7 @@ struct mcpi_space_s {
     cudaStream_t s_h2d = nullptr, s_d2h = nullptr;
     double2 *d_hin[2] = {nullptr, nullptr}, *d_hout[2] = {nullptr, nullptr};
     cudaEvent_t ev_in[2] = {nullptr, nullptr}, ev_comp[2] = {nullptr, nullptr}, ev_out[2] = {nullptr, nullptr};
+    bool host_pipe_ready = false;    // set only once every resource above exists
     uint32_t *d_W = nullptr;
     double *d_sq = nullptr;
     bool has_op = false;

@@ -27,7 +27,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORC_PATH = os.path.join(HERE, "liborc.so")
 REF_PATH = os.path.join(HERE, "_ref", "libmcpi_ref.so")
-REFERENCE_SRC = os.environ.get("MCPI_REFERENCE_SRC", "/root/reference")
+# the reference source tree: MCPI_REFERENCE_SRC, else "reference" beside the repository
+REFERENCE_SRC = os.environ.get(
+    "MCPI_REFERENCE_SRC", os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference"))
 
 _c_int_p = ct.POINTER(ct.c_int32)
 _c_i64_p = ct.POINTER(ct.c_int64)

@@ -18,12 +18,3 @@ def test_fock_index_arithmetic(tmp_path):
     r = subprocess.run([str(exe), "large"], capture_output=True, text=True)
     assert r.returncode == 0 and r.stdout.strip() == "ok", r.stdout + r.stderr
 
-
-def test_staging_ranges(tmp_path):
-    """tests/cpp/staging_check.cpp: the per-block E ranges of the TMA-staged
-    pair-creation kernel are gap-free, inside E, and fit the staging buffer."""
-    exe = tmp_path / "staging_check"
-    subprocess.run(["g++", "-O2", "-std=c++17", os.path.join(ROOT, "tests", "cpp", "staging_check.cpp"),
-                    "-o", str(exe)], check=True)
-    r = subprocess.run([str(exe)], capture_output=True, text=True)
-    assert r.returncode == 0 and r.stdout.strip() == "ok", r.stdout + r.stderr

@@ -37,8 +37,13 @@ def _static(N, M, Ho, Hint, C, variant=mc.VARIANT_MAPS):
     return rc, out.cpu().numpy()
 
 
-def _regular(N, M, Ho, Hint, C, variant=mc.VARIANT_MAPS):
+def _regular(N, M, Ho, Hint, C, variant=mc.VARIANT_MAPS, same_kernels=False):
     sp = mc.FockSpace(N, M)
+    if same_kernels:
+        # the compressed-row pair kernel and index decoding, as the static path runs
+        for opt in (mc.OPT_DENSE_PAIR_KERNEL, mc.OPT_NO_MOMENTUM_KERNEL, mc.OPT_NO_GEMM_KERNEL,
+                    mc.OPT_NO_OCC_TABLES):
+            sp.set_option(opt, 1)
     sp.set_integrals(Ho, Hint, variant)
     out = sp.apply_h(C).cpu().numpy()
     sp.close()
@@ -85,3 +90,44 @@ def test_static_rejects_oversize():
     rc = f(3, 11, np.zeros(121, np.complex128).ctypes.data, np.zeros(11 ** 4, np.complex128).ctypes.data,
            mc.VARIANT_MAPS, x.data_ptr(), y.data_ptr(), None)
     assert rc == 2   # M beyond the static path's limit
+
+
+def test_static_folds_the_same_pair_matrix():
+    # both paths fold the integrals with one shared routine: with the regular
+    # space held to the same kernels the two results agree bit for bit
+    for N, M, variant in [(8, 8, mc.VARIANT_MAPS), (7, 6, mc.VARIANT_HASH)]:
+        C, Ho, Hint = mc.random_problem(N, M, 75)
+        for _ in range(2):
+            rc, got = _static(N, M, Ho, Hint, C, variant)
+            assert rc == 0
+            assert np.array_equal(got, _regular(N, M, Ho, Hint, C, variant, same_kernels=True)), (N, M)
+
+
+def test_static_refuses_stream_capture():
+    # a call on a capturing stream returns MCPI_ERR_ARG with nothing enqueued,
+    # and the caller's graph still captures and replays
+    N, M = 6, 5
+    C, Ho, Hint = mc.random_problem(N, M, 76)
+    rc, ref = _static(N, M, Ho, Hint, C)
+    assert rc == 0
+    f = mc.lib().mcpi_apply_h_static
+    Ho = np.ascontiguousarray(Ho, np.complex128)
+    Hint = np.ascontiguousarray(Hint, np.complex128)
+    x = torch.from_numpy(np.ascontiguousarray(C, np.complex128)).cuda()
+    out = torch.zeros_like(x)
+    y = torch.zeros(16, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        y.add_(1.0)
+        rc = f(N, M, Ho.ctypes.data, Hint.ctypes.data, mc.VARIANT_MAPS, x.data_ptr(), out.data_ptr(),
+               ct.c_void_p(torch.cuda.current_stream().cuda_stream))
+        y.add_(1.0)
+    assert rc == 1   # MCPI_ERR_ARG
+    g.replay()
+    torch.cuda.synchronize()
+    assert torch.all(y == 2.0).item()
+    assert torch.count_nonzero(out).item() == 0          # nothing of the refused call ran
+    rc, again = _static(N, M, Ho, Hint, C)               # outside the capture it works again
+    assert rc == 0 and np.array_equal(again, ref)
+    del g
