@@ -88,6 +88,17 @@ MCPI_API int mcpi_space_sync(mcpi_space sp);
  * kernels then decode every row index; 1 also frees existing tables). Takes
  * effect at the next mcpi_set_integrals. */
 #define MCPI_OPT_NO_OCC_TABLES 7
+/* MCPI_OPT_FUSED_HPSI (0/1, default 0): run H.psi with momentum-block
+ * integrals as one persistent kernel that interleaves the pair-annihilation
+ * and pair-creation tiles, so most of the P x NC(N-2,M) intermediate is read
+ * back from L2 instead of HBM (results are bitwise those of the two-kernel
+ * form; at N=16, M=10 it is slower: 0.365 against 0.300 ms). Whole-vector
+ * calls only; row ranges keep the two kernels. */
+#define MCPI_OPT_FUSED_HPSI 8
+/* MCPI_OPT_FUSED_LEAD (>= 0, default 128): producer tiles (256
+ * configurations of the N-2 space each) the fused kernel's schedule runs
+ * ahead of its consumers. */
+#define MCPI_OPT_FUSED_LEAD 9
 MCPI_API int mcpi_space_set_option(mcpi_space sp, int option, int value);
 MCPI_API int mcpi_space_dims(mcpi_space sp, int *N, int *M, int64_t *nc);
 /* Device memory on the space's device, and a synchronous copy in any direction
@@ -141,7 +152,9 @@ MCPI_API int mcpi_apply_h_rows(mcpi_space sp, const void *d_C, int64_t row0, int
 /* mcpi_apply_h, timed: runs it reps times with CUDA events around each of its
  * two kernels on the space's stream (synchronising after every repetition) and
  * returns their mean durations in ms: h_ms[0] pair annihilation + pair-matrix
- * kernel, h_ms[1] pair creation kernel. For measurement, not for production. */
+ * kernel, h_ms[1] pair creation kernel (with MCPI_OPT_FUSED_HPSI on and
+ * momentum-block integrals: h_ms[0] the fused kernel, h_ms[1] = 0). For
+ * measurement, not for production. */
 MCPI_API int mcpi_apply_h_profile(mcpi_space sp, const void *d_C, void *d_out, int reps, float *h_ms);
 /* out = H C without allocating anything. No counterpart in the reference.
  * For callers that cannot allocate device memory where they need H.psi (a

@@ -39,6 +39,8 @@ OPT_NO_GEMM_KERNEL = 4
 OPT_WAIT_LIMIT_KCYCLES = 5
 OPT_TEST_STALL_GATHER = 6
 OPT_NO_OCC_TABLES = 7
+OPT_FUSED_HPSI = 8
+OPT_FUSED_LEAD = 9
 
 
 class MCPIError(RuntimeError):

@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <complex>
 #include <cstdarg>
@@ -263,11 +264,80 @@ int reserve(void *&ptr, size_t &cap, size_t bytes)
     return MCPI_OK;
 }
 
+int ensure_fused(mcpi_space_s *sp);
+
 int ensure_E(mcpi_space_s *sp)
 {
-    if (sp->N < 2 || sp->d_E) return MCPI_OK;
-    CK(cudaMalloc(&sp->d_E, sizeof(double2) * (size_t)sp->P * sp->nc2));
+    if (sp->N < 2) return MCPI_OK;
+    if (!sp->d_E) CK(cudaMalloc(&sp->d_E, sizeof(double2) * (size_t)sp->P * sp->nc2));
+    return ensure_fused(sp);
+}
+
+void free_fused(mcpi_space_s *sp)
+{
+    if (sp->d_fz) {
+        cudaStreamSynchronize(sp->stream);
+        cudaFree(sp->d_fz);
+    }
+    sp->d_fz = nullptr;
+    sp->fz = mcpi::FusedPlan{};
+    sp->fz_ready = false;
+}
+
+// Builds the fused H.psi schedule of the space (FusedPlan, kernels.h): the
+// highest producer tile each consumer tile reads, from the device, then the
+// order -- before consumer tile c every producer tile up to need[c] + lead
+// not yet listed, then c. Once per space (and after an option change).
+int ensure_fused(mcpi_space_s *sp)
+{
+    if (!sp->fused_on || sp->fz_ready || sp->N < 2 || sp->M < 2) return MCPI_OK;
+    const int64_t T = mcpi::kFusedTile;
+    const int np = (int)((sp->nc2 + T - 1) / T), nct = (int)((sp->nc + T - 1) / T);
+    const int ngroups = (np + mcpi::kFusedGroup - 1) / mcpi::kFusedGroup;
+    // need | order | ctl (128-byte aligned) | count
+    const size_t oc = ((size_t)nct + np + nct + 31) & ~size_t(31);
+    const size_t words = oc + mcpi::kFusedCtlWords + ngroups;
+    free_fused(sp);
+    CK(cudaMalloc(&sp->d_fz, sizeof(int) * words));
+    int *need = sp->d_fz, *order = need + nct;
+    unsigned *ctl = (unsigned *)(sp->d_fz + oc), *count = ctl + mcpi::kFusedCtlWords;
+    CK(cudaMemsetAsync(ctl, 0, sizeof(unsigned) * ((size_t)mcpi::kFusedCtlWords + ngroups), sp->stream));
+    CK(mcpi::launch_fused_need(sp->sp, sp->tables(), need, sp->stream));
+    std::vector<int> h_need(nct), h_order;
+    h_order.reserve((size_t)np + nct);
+    CK(cudaMemcpyAsync(h_need.data(), need, sizeof(int) * nct, cudaMemcpyDeviceToHost, sp->stream));
+    CK(cudaStreamSynchronize(sp->stream));
+    int next = 0;
+    for (int c = 0; c < nct; ++c) {
+        if (h_need[c] < 0 || h_need[c] >= np) return fail(MCPI_ERR_CUDA, "fused schedule: bad tile %d", h_need[c]);
+        const int upto = std::min(np - 1, h_need[c] + sp->fused_lead);
+        while (next <= upto) h_order.push_back(next++);
+        h_order.push_back(-1 - c);
+    }
+    while (next < np) h_order.push_back(next++);
+    CK(cudaMemcpyAsync(order, h_order.data(), sizeof(int) * h_order.size(), cudaMemcpyHostToDevice, sp->stream));
+    int grid = 0;
+    size_t smem = 0;
+    CK(mcpi::fused_config(sp->sp, &grid, &smem));
+    CK(cudaStreamSynchronize(sp->stream));   // h_order goes out of scope
+    sp->fz.order = order;
+    sp->fz.nitems = (int)h_order.size();
+    sp->fz.need = need;
+    sp->fz.count = count;
+    sp->fz.ctl = ctl;
+    sp->fz.np = np;
+    sp->fz.grid = grid;
+    sp->fz_ready = true;
     return MCPI_OK;
+}
+
+// The launch view of a pair operator, with the space's fused schedule
+// attached when the fused form is on and built.
+PairOp op_view(const mcpi_space_s *sp, const DevPairOp &op)
+{
+    PairOp v = op.view();
+    if (sp->fused_on && sp->fz_ready) v.fused = sp->fz;
+    return v;
 }
 
 int ensure_gram(mcpi_space_s *sp)
@@ -291,7 +361,7 @@ int apply_op(mcpi_space_s *sp, const DevPairOp &op, const void *d_C, void *d_out
     DeviceGuard g(sp->device);
     int rc = ensure_E(sp);
     if (rc) return rc;
-    CK(mcpi::launch_apply_h(sp->sp, sp->tables(), op.view(), op.blocks(), (const double2 *)d_C,
+    CK(mcpi::launch_apply_h(sp->sp, sp->tables(), op_view(sp, op), op.blocks(), (const double2 *)d_C,
                             sp->d_E, (double2 *)d_out, sp->stream));
     return MCPI_OK;
 }
@@ -459,6 +529,7 @@ int mcpi_space_destroy(mcpi_space sp)
     cudaFree(sp->d_lzblk);
     cudaFree(sp->d_lzr);
     free_host_pipe(sp);
+    free_fused(sp);
     if (sp->own) cudaStreamDestroy(sp->own);
     delete sp;
     return MCPI_OK;
@@ -497,6 +568,15 @@ int mcpi_space_set_option(mcpi_space sp, int option, int value)
     case MCPI_OPT_TEST_STALL_GATHER:
         sp->test_stall = value != 0;
         sp->fwd.test_stall = sp->adj.test_stall = sp->test_stall;
+        return MCPI_OK;
+    case MCPI_OPT_FUSED_HPSI:
+        if ((value != 0) != sp->fused_on) free_fused(sp);
+        sp->fused_on = value != 0;
+        return MCPI_OK;
+    case MCPI_OPT_FUSED_LEAD:
+        if (value < 0) return fail(MCPI_ERR_ARG, "fused lead must be >= 0");
+        if (value != sp->fused_lead) free_fused(sp);
+        sp->fused_lead = value;
         return MCPI_OK;
     case MCPI_OPT_CREATE_FORM:
         sp->create_form = value;
@@ -761,7 +841,7 @@ int mcpi_apply_h_host(mcpi_space sp, int count, const void *const *h_C, void *co
         CK(cudaEventRecord(sp->ev_in[b], sp->s_h2d));
         CK(cudaStreamWaitEvent(sp->stream, sp->ev_in[b], 0));
         if (k >= 2) CK(cudaStreamWaitEvent(sp->stream, sp->ev_out[b], 0));
-        CK(mcpi::launch_apply_h(sp->sp, sp->tables(), sp->fwd.view(), sp->fwd.blocks(), sp->d_hin[b], sp->d_E,
+        CK(mcpi::launch_apply_h(sp->sp, sp->tables(), op_view(sp, sp->fwd), sp->fwd.blocks(), sp->d_hin[b], sp->d_E,
                                 sp->d_hout[b], sp->stream));
         CK(cudaEventRecord(sp->ev_comp[b], sp->stream));
         CK(cudaStreamWaitEvent(sp->s_d2h, sp->ev_comp[b], 0));
@@ -784,7 +864,22 @@ int mcpi_apply_h_profile(mcpi_space sp, const void *d_C, void *d_out, int reps, 
     for (auto &e : ev) CK(cudaEventCreate(&e));
     float tot[2] = {0.f, 0.f};
     cudaError_t e = cudaSuccess;
-    for (int r = 0; r < reps && e == cudaSuccess; ++r) {
+    const PairOp fop = op_view(sp, sp->fwd);
+    if (fop.fused.order && sp->fwd.hblk) {
+        // fused form: one kernel, reported as h_ms[0]
+        for (int r = 0; r < reps && e == cudaSuccess; ++r) {
+            e = cudaEventRecord(ev[0], sp->stream);
+            if (e == cudaSuccess)
+                e = mcpi::launch_apply_h(sp->sp, sp->tables(), fop, sp->fwd.blocks(), (const double2 *)d_C,
+                                         sp->d_E, (double2 *)d_out, sp->stream, 3);
+            if (e == cudaSuccess) e = cudaEventRecord(ev[1], sp->stream);
+            if (e == cudaSuccess) e = cudaEventSynchronize(ev[1]);
+            float a = 0.f;
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&a, ev[0], ev[1]);
+            tot[0] += a;
+        }
+    }
+    for (int r = 0; r < reps && e == cudaSuccess && !(fop.fused.order && sp->fwd.hblk); ++r) {
         e = cudaEventRecord(ev[0], sp->stream);
         if (e == cudaSuccess)
             e = mcpi::launch_apply_h(sp->sp, sp->tables(), sp->fwd.view(), sp->fwd.blocks(),
@@ -888,7 +983,7 @@ int mcpi_lanczos(mcpi_space sp, void *d_lvec, int lm, double *h_diag, double *h_
     s.nparts = mcpi::lanczos_parts(nc);
     const int init[2] = {0, lm};
     double2 *V = (double2 *)d_lvec;
-    const PairOp op = sp->fwd.view();
+    const PairOp op = op_view(sp, sp->fwd);
     const mcpi::BlockOp bo = sp->fwd.blocks();
     const SpaceTables tb = sp->tables();
     e = cudaMemsetAsync(blk, 0, bytes, sp->stream);
@@ -1007,7 +1102,7 @@ int mcpi_ground_lowmem(mcpi_space sp, void *d_C, int niter, double *E0, int *ite
     s.iters = s.done + 1;
     s.nparts = mcpi::lanczos_parts(nc);
     double2 *v[2] = {vec, vec + nc}, *r = vec + 2 * nc, *acc = vec + 3 * nc;
-    const PairOp op = sp->fwd.view();
+    const PairOp op = op_view(sp, sp->fwd);
     const mcpi::BlockOp bo = sp->fwd.blocks();
     const SpaceTables tb = sp->tables();
     const int init[2] = {0, lm};

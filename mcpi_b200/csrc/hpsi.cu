@@ -629,24 +629,76 @@ __global__ void __launch_bounds__(kT1b) k_pair_annihilate_blocks(Space sp, Space
 // index below is a compile-time constant, so its reads are constant-bank
 // operands. Otherwise hblk is global memory and the values are staged in
 // shared memory.
-template <int M, bool PARAM = false>
-__device__ __forceinline__ void annihilate_momentum_body(const Space &sp, const SpaceTables &tb,
-                                                         const double2 *__restrict__ hblk, int nh,
-                                                         const double2 *__restrict__ psi,
-                                                         double2 *__restrict__ E, uint32_t block)
-{
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    double2 *hs = reinterpret_cast<double2 *>(smem_raw);          // nh (staged form only)
-    double *sq = reinterpret_cast<double *>(hs + (PARAM ? 0 : nh)); // wstride
-    uint32_t *W = reinterpret_cast<uint32_t *>(sq + sp.wstride);  // (M-1) x wstride
-    load_tables(sp, tb, W, sq);
-    if (!PARAM)
-        for (int x = threadIdx.x; x < nh; x += blockDim.x) hs[x] = hblk[x];
-    const double2 *hv = PARAM ? hblk : hs;
-    __syncthreads();
+// How E entries are stored and loaded. The two-kernel path streams E through
+// (evict-first stores and loads: it does not fit in L2); the fused path keeps
+// it in L2 between its producer and consumer tiles.
+enum : int {
+    kEStoreStream = 0,     // st.global.cs
+    kEStorePlain = 1,      // st.global (write-back)
+    kEStoreKeep = 2,       // st.global with an L2 evict_last cache policy
+};
+enum : int {
+    kELoadStream = 0,      // ld.global.cs
+    kELoadDrop = 1,        // ld.global.cg with an L2 evict_first cache policy
+    kELoadL2 = 2,          // ld.global.cg
+};
 
-    const uint32_t m = block * kT2 + threadIdx.x;
-    if (m >= sp.nc2) return;
+__device__ __forceinline__ uint64_t l2_policy_evict_last()
+{
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;\n" : "=l"(p));
+    return p;
+}
+
+__device__ __forceinline__ uint64_t l2_policy_evict_first()
+{
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;\n" : "=l"(p));
+    return p;
+}
+
+template <int EST>
+__device__ __forceinline__ void store_e(double2 *a, double2 v, uint64_t pol)
+{
+    if constexpr (EST == kEStoreStream) {
+        __stcs(a, v);
+    } else if constexpr (EST == kEStorePlain) {
+        *a = v;
+    } else {
+        asm volatile("st.global.L2::cache_hint.v2.f64 [%0], {%1, %2}, %3;\n" ::"l"(a), "d"(v.x), "d"(v.y),
+                     "l"(pol)
+                     : "memory");
+    }
+}
+
+template <int ELD>
+__device__ __forceinline__ double2 load_e(const double2 *a, uint64_t pol)
+{
+    if constexpr (ELD == kELoadStream) {
+        return __ldcs(a);
+    } else if constexpr (ELD == kELoadL2) {
+        return __ldcg(a);
+    } else {
+        double2 v;
+        asm volatile("ld.global.cg.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;\n"
+                     : "=d"(v.x), "=d"(v.y)
+                     : "l"(a), "l"(pol));
+        return v;
+    }
+}
+
+// One (N-2)-configuration m of kernel 1, momentum-block form: gathers its
+// values <m|a_q a_l|psi> block by block and writes E[a][m] for every pair a.
+// W, sq: the space's tables (shared memory); hv: the block values.
+// ESTN / ESTF: store flavour of the pairs a = (k <= s) with s < FAR (near) and
+// s >= FAR (far).
+template <int M, int ESTN, int ESTF = ESTN, int FAR = M>
+__device__ __forceinline__ void annihilate_momentum_row(const Space &sp, const SpaceTables &tb,
+                                                        const uint32_t *W, const double *sq,
+                                                        const double2 *__restrict__ hv,
+                                                        const double2 *__restrict__ psi,
+                                                        double2 *__restrict__ E, uint32_t m, uint64_t pol)
+{
     const int ws = sp.wstride;
     int u[M], Q[M];
     occupations<M>(tb.occ2, tb.occ_bits, m, sp.N - 2, sp.nc2, W, ws, u, Q);
@@ -688,10 +740,35 @@ __device__ __forceinline__ void annihilate_momentum_body(const Space &sp, const 
 #pragma unroll
                 for (int c = 0; c < NB; ++c)
                     if (c < n) cfma(e, hv[off + r * n + c], d[c]);
-                __stcs(E + (size_t)pair_index(qlo + r, K - qlo - r, M) * stride + m, e);
+                double2 *dst = E + (size_t)pair_index(qlo + r, K - qlo - r, M) * stride + m;
+                if (K - qlo - r >= FAR)
+                    store_e<ESTF>(dst, e, pol);
+                else
+                    store_e<ESTN>(dst, e, pol);
             }
         off += n * n;
     }
+}
+
+template <int M, bool PARAM = false>
+__device__ __forceinline__ void annihilate_momentum_body(const Space &sp, const SpaceTables &tb,
+                                                         const double2 *__restrict__ hblk, int nh,
+                                                         const double2 *__restrict__ psi,
+                                                         double2 *__restrict__ E, uint32_t block)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2 *hs = reinterpret_cast<double2 *>(smem_raw);          // nh (staged form only)
+    double *sq = reinterpret_cast<double *>(hs + (PARAM ? 0 : nh)); // wstride
+    uint32_t *W = reinterpret_cast<uint32_t *>(sq + sp.wstride);  // (M-1) x wstride
+    load_tables(sp, tb, W, sq);
+    if (!PARAM)
+        for (int x = threadIdx.x; x < nh; x += blockDim.x) hs[x] = hblk[x];
+    const double2 *hv = PARAM ? hblk : hs;
+    __syncthreads();
+
+    const uint32_t m = block * kT2 + threadIdx.x;
+    if (m >= sp.nc2) return;
+    annihilate_momentum_row<M, kEStoreStream>(sp, tb, W, sq, hv, psi, E, m, 0);
 }
 
 template <int M>
@@ -807,29 +884,20 @@ __global__ void __launch_bounds__(kT2, 4) k_pair_create(Space sp, SpaceTables tb
 // pair), 0.21 ms forcing five blocks per SM (spills); staging each block's
 // contiguous E ranges in shared memory with TMA bulk copies (0.73 ms) or
 // prefetching them into L2 (0.28 ms) was slower still.
-template <int M>
-__device__ __forceinline__ void create_smem_body(const Space &sp, const SpaceTables &tb,
-                                                 const double2 *__restrict__ hdiag,
-                                                 const double2 *__restrict__ psi,
-                                                 const double2 *__restrict__ E,
-                                                 double2 *__restrict__ out, uint32_t block,
-                                                 uint32_t row0, uint32_t row1)
+// One N-configuration i of kernel 2, shared-table form: row tables into this
+// thread's shared-memory columns (r1, Xr, Yr, vb), then the gathers. row:
+// i is a row to compute (out[i - row0]). ELDN / ELDF: how E is loaded for the
+// pairs (k <= s) with s < FAR and s >= FAR. STREAM_OUT: write out with an
+// evict-first store.
+template <int M, int ELDN, int ELDF = ELDN, int FAR = M, bool STREAM_OUT = false>
+__device__ __forceinline__ void create_row(const Space &sp, const SpaceTables &tb, const uint32_t *W,
+                                           const double *sq, const double2 *hd,
+                                           const double2 *__restrict__ psi, const double2 *E,
+                                           double2 *__restrict__ out, uint32_t i, bool row, uint32_t row0,
+                                           double *r1, uint32_t *Xr, uint32_t *Yr, unsigned char *vb,
+                                           uint64_t pol)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    double *r1 = reinterpret_cast<double *>(smem_raw);             // M x kTC
-    uint32_t *Xr = reinterpret_cast<uint32_t *>(r1 + M * kTC);     // M x kTC
-    uint32_t *Yr = Xr + M * kTC;                                   // M x kTC
-    unsigned char *vb = reinterpret_cast<unsigned char *>(Yr + M * kTC);   // M x kTC
-    double2 *hd = reinterpret_cast<double2 *>(vb + ((M * kTC + 15) & ~15)); // M
-    double *sq = reinterpret_cast<double *>(hd + M);               // wstride
-    uint32_t *W = reinterpret_cast<uint32_t *>(sq + sp.wstride);   // (M-1) x wstride
-    load_tables(sp, tb, W, sq);
-    if (threadIdx.x < M) hd[threadIdx.x] = hdiag[threadIdx.x];
-    __syncthreads();
-
     const int t = threadIdx.x;
-    const uint32_t i = row0 + block * kTC + t;   // rows [row0, row1) -> out[i - row0]
-    const bool row = i < row1;
     const int ws = sp.wstride;
     double2 acc;
     {
@@ -885,7 +953,10 @@ __device__ __forceinline__ void create_smem_body(const Space &sp, const SpaceTab
                 const uint32_t mm = Xr[k * kTC + t] - Yr[s * kTC + t];
                 cc[j] = c;
                 // empty pairs (c = 0: their index is meaningless) load nothing
-                ee[j] = c != 0.0 ? __ldcs(E + (size_t)p * stride + mm) : make_double2(0.0, 0.0);
+                const double2 *src = E + (size_t)p * stride + mm;
+                ee[j] = c == 0.0     ? make_double2(0.0, 0.0)
+                        : s >= FAR   ? load_e<ELDF>(src, pol)
+                                     : load_e<ELDN>(src, pol);
             }
         }
 #pragma unroll
@@ -895,7 +966,44 @@ __device__ __forceinline__ void create_smem_body(const Space &sp, const SpaceTab
                 acc.y = fma(cc[j], ee[j].y, acc.y);
             }
     }
-    out[i - row0] = acc;
+    if constexpr (STREAM_OUT)
+        __stcs(out + (i - row0), acc);
+    else
+        out[i - row0] = acc;
+}
+
+// Kernel 2, shared-table form (default): the per-row tables (Xr, Yr, sqrt v_k
+// and v_k - 1) live in shared-memory columns that only their thread touches,
+// so the pair loop needs few registers (no spills) and occupancy is set by
+// shared memory (17 bytes per orbital and row). Measured at N=16, M=10:
+// 0.183 ms with the E gathers issued in groups of 8 (0.198 ms consumed one by
+// one, 0.186 ms in groups of 16), against 0.238 ms with two double tables, 0.248 ms for the register
+// form, 0.216 ms keeping only occupation bytes (square roots looked up per
+// pair), 0.21 ms forcing five blocks per SM (spills); staging each block's
+// contiguous E ranges in shared memory with TMA bulk copies (0.73 ms) or
+// prefetching them into L2 (0.28 ms) was slower still.
+template <int M>
+__device__ __forceinline__ void create_smem_body(const Space &sp, const SpaceTables &tb,
+                                                 const double2 *__restrict__ hdiag,
+                                                 const double2 *__restrict__ psi,
+                                                 const double2 *__restrict__ E,
+                                                 double2 *__restrict__ out, uint32_t block,
+                                                 uint32_t row0, uint32_t row1)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double *r1 = reinterpret_cast<double *>(smem_raw);             // M x kTC
+    uint32_t *Xr = reinterpret_cast<uint32_t *>(r1 + M * kTC);     // M x kTC
+    uint32_t *Yr = Xr + M * kTC;                                   // M x kTC
+    unsigned char *vb = reinterpret_cast<unsigned char *>(Yr + M * kTC);   // M x kTC
+    double2 *hd = reinterpret_cast<double2 *>(vb + ((M * kTC + 15) & ~15)); // M
+    double *sq = reinterpret_cast<double *>(hd + M);               // wstride
+    uint32_t *W = reinterpret_cast<uint32_t *>(sq + sp.wstride);   // (M-1) x wstride
+    load_tables(sp, tb, W, sq);
+    if (threadIdx.x < M) hd[threadIdx.x] = hdiag[threadIdx.x];
+    __syncthreads();
+
+    const uint32_t i = row0 + block * kTC + threadIdx.x;   // rows [row0, row1) -> out[i - row0]
+    create_row<M, kELoadStream>(sp, tb, W, sq, hd, psi, E, out, i, i < row1, row0, r1, Xr, Yr, vb, 0);
 }
 
 template <int M>
@@ -908,6 +1016,256 @@ __global__ void __launch_bounds__(kTC, 4) k_pair_create_smem(Space sp, SpaceTabl
     // blocks run from the top rows down: their E entries (images near the end of
     // each E row) are the ones kernel 1 wrote last, some still in L2
     create_smem_body<M>(sp, tb, op.hdiag, psi, E, out, gridDim.x - 1 - blockIdx.x, row0, row1);
+}
+
+// ---------------------------------------------------------------------------
+// Fused H.psi, momentum-block form (FusedPlan in kernels.h). The two-kernel
+// path writes all of E (P x NC(N-2,M) complex, 719 MB at N=16, M=10) to HBM
+// and reads it back. Here one persistent grid walks kernel 1's tiles and
+// kernel 2's tiles in one order: consumer tile c (rows in index order) comes
+// right after the producer tiles up to need[c]. For a fixed pair a the map
+// v -> v - e_k - e_s keeps the index order, so the E columns a consumer reads
+// lie just behind the producer front, and the E alive between its write and
+// its read stays in L2 (peak 53 MB, mean 19 MB at N=16, M=10, against 126 MB).
+//
+// Hand-over: producer tiles are counted in groups of kFusedGroup; a producer
+// block stores its E, then (thread 0, after a barrier and a device-scope
+// fence) adds one to its group's counter. A consumer's thread 0 waits until
+// every group up to need[c] / kFusedGroup is complete (acquire loads; it
+// remembers the groups it has seen complete, so each group is checked by a
+// block at most until it is), then the block reads. Items are handed out in
+// order from a ticket counter and producers never wait, so every tile a
+// consumer waits for belongs to a running block: the waits end. A block grabs
+// its next ticket early -- at the start of a producer tile, or once a
+// consumer's wait is over -- never while it may still wait, so a held ticket
+// always belongs to a block that will reach it. The waits are bounded all the
+// same (about two seconds): one that runs out sets the abort word and the
+// status word and its block skips the tile (out is then invalid; the next
+// synchronising call reports MCPI_ERR_TIMEOUT); every later consumer sees the
+// abort word and skips at once. test_stall (a test switch) keeps the
+// producers from counting, so that the waits run out. The last block to leave
+// zeroes the counters for the next call (or graph replay).
+//
+// Each consumer row does exactly the arithmetic of kernel 2 on exactly the
+// values kernel 1 writes, so the fused result is bitwise the two-kernel one.
+//
+// Which pairs stay in L2. A pair a = (k, s) that includes the top orbital
+// (s = M-1) moves a configuration a whole slab of the index order (the top
+// occupation is the most significant digit), so its E column is read about
+// a slab after it is written: at N=16, M=10 those 10 of the 55 pairs account
+// for 15 of the 19 MB mean live window. They are written and read as in the
+// two-kernel form (evict-first streaming, through HBM); the other pairs are
+// stored with an evict-last and loaded with an evict-first L2 policy (mean
+// live window 4 MB).
+//
+// Measured (N=16, M=10, Lieb, B200): 0.365 ms per H.psi at a lead of 192
+// tiles against 0.300 ms for the two kernels. DRAM traffic falls from about
+// 1.5 GB to 1.1 GB -- the reads of E mostly hit L2, but every dirty E line is
+// still written back when L2 evicts it -- while the kernel is bound by
+// latency and barriers at three blocks per SM (80 registers; four blocks
+// spill and run at 0.41 ms). So the two-kernel form stays the default.
+// ---------------------------------------------------------------------------
+// control words, each on its own 128-byte line (FusedPlan::ctl)
+enum : int { kFzTicket = 0, kFzExited = 32, kFzAbort = 64 };
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *a)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];\n" : "=r"(v) : "l"(a) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ unsigned ld_volatile_u32(const unsigned *a)
+{
+    return *reinterpret_cast<const volatile unsigned *>(a);
+}
+
+__device__ __forceinline__ int fused_item(const FusedPlan &fz, unsigned k)
+{
+    return k < (unsigned)fz.nitems ? fz.order[k] : INT_MIN;
+}
+
+template <int M>
+__global__ void __launch_bounds__(kTC, 3)
+    k_hpsi_fused(Space sp, SpaceTables tb, const __grid_constant__ MomBlocks<M> hp,
+                 const double2 *__restrict__ hdiag, const double2 *__restrict__ psi, double2 *E,
+                 double2 *__restrict__ out, FusedPlan fz, int *status, long long wait_cycles, int test_stall)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double *r1 = reinterpret_cast<double *>(smem_raw);             // M x kTC
+    uint32_t *Xr = reinterpret_cast<uint32_t *>(r1 + M * kTC);     // M x kTC
+    uint32_t *Yr = Xr + M * kTC;                                   // M x kTC
+    unsigned char *vb = reinterpret_cast<unsigned char *>(Yr + M * kTC);   // M x kTC
+    double2 *hd = reinterpret_cast<double2 *>(vb + ((M * kTC + 15) & ~15)); // M
+    double *sq = reinterpret_cast<double *>(hd + M);               // wstride
+    uint32_t *W = reinterpret_cast<uint32_t *>(sq + sp.wstride);   // (M-1) x wstride
+    __shared__ int s_item[2];
+    __shared__ int s_ok;
+    const int t = threadIdx.x;
+    load_tables(sp, tb, W, sq);
+    if (t < M) hd[t] = hdiag[t];
+    if (t == 0) s_item[0] = fused_item(fz, atomicAdd(fz.ctl + kFzTicket, 1u));
+    __syncthreads();
+
+    const long long limit = wait_cycles > 0 ? wait_cycles : kWaitCycles;
+    const int ngroups = (fz.np + kFusedGroup - 1) / kFusedGroup;
+    const uint64_t pst = l2_policy_evict_last(), pld = l2_policy_evict_first();
+    int known = 0;   // (thread 0) producer groups below this are known to be complete
+
+    for (int it = 0;; ++it) {
+        const int item = s_item[it & 1];
+        if (item == INT_MIN) break;
+        unsigned ticket = 0;   // (thread 0) the next item's ticket, taken early, used at the end
+        if (item >= 0) {
+            // producer: kernel 1 on configurations [item * 256, item * 256 + 256)
+            if (t == 0) ticket = atomicAdd(fz.ctl + kFzTicket, 1u);
+            const uint32_t m = (uint32_t)item * kFusedTile + t;
+            if (m < sp.nc2)
+                annihilate_momentum_row<M, kEStoreKeep, kEStoreStream, M - 1>(sp, tb, W, sq, hp.v, psi, E, m, pst);
+            __syncthreads();
+            if (t == 0) {
+                if (!test_stall) {
+                    __threadfence();
+                    atomicAdd(fz.count + item / kFusedGroup, 1u);
+                }
+                s_item[(it + 1) & 1] = fused_item(fz, ticket);
+            }
+        } else {
+            // consumer: kernel 2 on rows [c * 256, c * 256 + 256)
+            const int c = -1 - item;
+            if (t == 0) {
+                const int gneed = fz.need[c] / kFusedGroup;
+                int ok = 1;
+                const long long t0 = clock64();
+                while (known <= gneed) {
+                    const unsigned full = known + 1 < ngroups ? kFusedGroup : fz.np - known * kFusedGroup;
+                    if (ld_acquire_u32(fz.count + known) == full) {
+                        ++known;
+                        continue;
+                    }
+                    if (ld_volatile_u32(fz.ctl + kFzAbort)) {
+                        ok = 0;
+                        break;
+                    }
+                    if (clock64() - t0 > limit) {
+                        atomicExch(fz.ctl + kFzAbort, 1u);
+                        if (status) atomicExch(status, 1);
+                        ok = 0;
+                        break;
+                    }
+                    __nanosleep(200);
+                }
+                __threadfence();
+                s_ok = ok;
+                // the wait is over: this block reaches its next item in bounded time
+                ticket = atomicAdd(fz.ctl + kFzTicket, 1u);
+            }
+            __syncthreads();
+            if (s_ok) {
+                const uint32_t i = (uint32_t)c * kFusedTile + t;
+                create_row<M, kELoadDrop, kELoadStream, M - 1, true>(sp, tb, W, sq, hd, psi, E, out, i, i < sp.nc,
+                                                                      0u, r1, Xr, Yr, vb, pld);
+            }
+            if (t == 0) s_item[(it + 1) & 1] = fused_item(fz, ticket);
+        }
+        __syncthreads();   // the next item is visible; s_ok is free again
+    }
+    // the last block out zeroes the counters for the next call
+    __shared__ int s_last;
+    if (t == 0) {
+        __threadfence();
+        s_last = atomicAdd(fz.ctl + kFzExited, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (s_last) {
+        __threadfence();
+        for (int g = t; g < ngroups; g += blockDim.x) fz.count[g] = 0u;
+        if (t == 0) {
+            fz.ctl[kFzTicket] = 0u;
+            fz.ctl[kFzAbort] = 0u;
+            fz.ctl[kFzExited] = 0u;
+        }
+        __threadfence();
+    }
+}
+
+// need[c]: the highest producer tile that consumer tile c reads. The largest
+// E column a row v reads is that of its two lowest particles (removing them
+// changes only the least significant occupations of the index order).
+template <int M>
+__global__ void __launch_bounds__(kFusedTile) k_fused_need(Space sp, SpaceTables tb, int *need)
+{
+    extern __shared__ uint32_t Wd[];   // (M-1) x wstride
+    __shared__ uint32_t s_max[kFusedTile / 32];
+    const int ws = sp.wstride;
+    for (int x = threadIdx.x; x < (M - 1) * ws; x += blockDim.x) Wd[x] = tb.W[x];
+    __syncthreads();
+    const uint32_t i = blockIdx.x * kFusedTile + threadIdx.x;
+    uint32_t mx = 0;
+    if (i < sp.nc) {
+        int v[M], P[M];
+        occupations<M>(tb.occ, tb.occ_bits, i, sp.N, sp.nc, Wd, ws, v, P);
+        int k0 = 0;
+        while (k0 < M - 1 && v[k0] == 0) ++k0;
+        int k1 = k0;
+        if (v[k0] < 2) {
+            k1 = k0 + 1;
+            while (k1 < M - 1 && v[k1] == 0) ++k1;
+        }
+        uint32_t A0[M], Am1[M], Am2[M];
+        prefix_table<M>(P, 0, Wd, ws, A0);
+        prefix_table<M>(P, -1, Wd, ws, Am1);
+        prefix_table<M>(P, -2, Wd, ws, Am2);
+        mx = idx_remove2(sp.nc2, A0, Am1, Am2, k0, k1, M);
+    }
+    for (int o = 16; o; o >>= 1) {
+        const uint32_t y = __shfl_down_sync(0xffffffffu, mx, o);
+        mx = y > mx ? y : mx;
+    }
+    if ((threadIdx.x & 31) == 0) s_max[threadIdx.x >> 5] = mx;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < kFusedTile / 32; ++w) mx = s_max[w] > mx ? s_max[w] : mx;
+        need[blockIdx.x] = (int)(mx / kFusedTile);
+    }
+}
+
+template <int M>
+cudaError_t fused_apply_m(const Space &sp, const SpaceTables &tb, const PairOp &op, const double2 *psi,
+                          double2 *E, double2 *out, cudaStream_t st)
+{
+    const size_t tab = sizeof(double) * sp.wstride + sizeof(uint32_t) * (M - 1) * sp.wstride;
+    const size_t sm = (sizeof(double) + 2 * sizeof(uint32_t)) * M * kTC + ((M * kTC + 15) & ~15) +
+                      sizeof(double2) * M + tab;
+    if (sm > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k_hpsi_fused<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e != cudaSuccess) return e;
+    }
+    MomBlocks<M> hp;
+    for (int x = 0; x < mom_values<M>(); ++x) hp.v[x] = op.hblk_host[x];
+    k_hpsi_fused<M><<<op.fused.grid, kTC, sm, st>>>(sp, tb, hp, op.hdiag, psi, E, out, op.fused, op.status,
+                                                   op.wait_cycles, op.test_stall);
+    return cudaGetLastError();
+}
+
+template <int M>
+cudaError_t fused_config_m(const Space &sp, int *grid, size_t *smem)
+{
+    const size_t tab = sizeof(double) * sp.wstride + sizeof(uint32_t) * (M - 1) * sp.wstride;
+    const size_t sm = (sizeof(double) + 2 * sizeof(uint32_t)) * M * kTC + ((M * kTC + 15) & ~15) +
+                      sizeof(double2) * M + tab;
+    const void *fn = (const void *)k_hpsi_fused<M>;
+    cudaError_t e = cudaSuccess;
+    if (sm > 48 * 1024 &&
+        (e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm)) != cudaSuccess)
+        return e;
+    int dev = 0, sms = 0, per = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, kTC, sm)) != cudaSuccess) return e;
+    *grid = sms * (per > 0 ? per : 1);
+    *smem = sm;
+    return cudaSuccess;
 }
 
 // ---------------------------------------------------------------------------
@@ -976,6 +1334,11 @@ cudaError_t apply_h_m(const Space &sp, const SpaceTables &tb, const PairOp &op, 
 {
     constexpr int P = M * (M + 1) / 2;
     const size_t tab = sizeof(double) * sp.wstride + sizeof(uint32_t) * (M - 1) * sp.wstride;
+    if constexpr (M >= 2) {
+        if (sp.N >= 2 && stages == 3 && op.fused.order && op.hblk_host && op.nhblk == mom_values<M>() &&
+            row0 == 0 && row1 == sp.nc && op.create_form == 0)
+            return fused_apply_m<M>(sp, tb, op, psi, E, out, st);
+    }
     if (sp.N >= 2 && (stages & 1) && op.hblk) {
         const unsigned g1 = (sp.nc2 + kT2 - 1) / kT2;
         if (op.hblk_host && op.nhblk == mom_values<M>()) {
@@ -1115,6 +1478,35 @@ size_t batch_smem(int M, int N, int nh, int stage)
 }
 
 int batch_rows_per_block(int stage) { return stage == 1 ? kT2 : kTC; }
+
+cudaError_t launch_fused_need(const Space &sp, const SpaceTables &tb, int *need, cudaStream_t st)
+{
+    if (sp.N < 2 || sp.M < 2) return cudaErrorInvalidValue;
+    const unsigned g = (sp.nc + kFusedTile - 1) / kFusedTile;
+    const size_t sm = sizeof(uint32_t) * (sp.M - 1) * sp.wstride;
+    switch (sp.M) {
+#define MCPI_CASE(m) \
+    case m: k_fused_need<m><<<g, kFusedTile, sm, st>>>(sp, tb, need); return cudaGetLastError();
+        MCPI_CASE(2) MCPI_CASE(3) MCPI_CASE(4) MCPI_CASE(5) MCPI_CASE(6) MCPI_CASE(7) MCPI_CASE(8)
+        MCPI_CASE(9) MCPI_CASE(10) MCPI_CASE(11) MCPI_CASE(12) MCPI_CASE(13) MCPI_CASE(14)
+        MCPI_CASE(15) MCPI_CASE(16)
+#undef MCPI_CASE
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t fused_config(const Space &sp, int *grid, size_t *smem)
+{
+    switch (sp.M) {
+#define MCPI_CASE(m) \
+    case m: return fused_config_m<m>(sp, grid, smem);
+        MCPI_CASE(2) MCPI_CASE(3) MCPI_CASE(4) MCPI_CASE(5) MCPI_CASE(6) MCPI_CASE(7) MCPI_CASE(8)
+        MCPI_CASE(9) MCPI_CASE(10) MCPI_CASE(11) MCPI_CASE(12) MCPI_CASE(13) MCPI_CASE(14)
+        MCPI_CASE(15) MCPI_CASE(16)
+#undef MCPI_CASE
+    default: return cudaErrorInvalidValue;
+    }
+}
 
 cudaError_t launch_apply_h(const Space &sp, const SpaceTables &tb, const PairOp &op,
                            const BlockOp &bo, const double2 *psi, double2 *E, double2 *out,

@@ -7,6 +7,26 @@
 
 namespace mcpi {
 
+// Fused H.psi (momentum-block form only). One persistent launch runs the
+// tiles of kernel 1 (producers: 256 (N-2)-configurations each, writing E) and
+// of kernel 2 (consumers: 256 rows each, reading E) in one interleaved order,
+// so that E is read back while it is still in L2 instead of making a round
+// trip through HBM. Blocks take items in that order from a ticket counter; a
+// consumer waits (bounded) until every producer tile up to need[c] has
+// counted itself done. Built once per space (capi.cpp: ensure_fused).
+constexpr int kFusedTile = 256;      // configurations per producer tile = rows per consumer tile
+constexpr int kFusedGroup = 16;      // producer tiles per completion counter
+constexpr int kFusedCtlWords = 96;   // ticket, exited, abort: one 128-byte line each
+struct FusedPlan {
+    const int *order = nullptr;  // nitems: producer tile p >= 0, or -1 - c for consumer tile c
+    int nitems = 0;
+    const int *need = nullptr;   // per consumer tile: the highest producer tile it reads
+    unsigned *count = nullptr;   // per group of kFusedGroup producer tiles: tiles done (zero between calls)
+    unsigned *ctl = nullptr;     // control words (zero between calls)
+    int np = 0;                  // producer tiles
+    int grid = 0;                // persistent blocks
+};
+
 // Two-body operator in pair form: H2 = sum_{a,b} Ht[a][b] A+_a A_b with
 // A_b = a_q a_l for the pair b = (q <= l). Stored as CSR over rows a.
 // hdiag[k] = Ho[k][k] (the diagonal one-body part, applied directly);
@@ -37,6 +57,8 @@ struct PairOp {
     // the block values as a kernel parameter (constant bank) instead of
     // staging them in shared memory
     const double2 *hblk_host;
+    // fused launch plan of the space (order == nullptr: two kernels)
+    FusedPlan fused;
 };
 constexpr int kGemmMaxP = 78;   // M <= 12: Ht (zero-padded to a multiple of 8 rows) fits shared memory
 
@@ -80,6 +102,12 @@ cudaError_t launch_apply_h(const Space &sp, const SpaceTables &tb, const PairOp 
                            const BlockOp &bo, const double2 *psi, double2 *E, double2 *out,
                            cudaStream_t st, int stages = 3, uint32_t row0 = 0,
                            uint32_t row1 = 0xffffffffu);
+
+// Fused H.psi set-up: need[c] = the highest producer tile consumer tile c
+// reads (device, ceil(nc / kFusedTile) entries); the persistent grid and
+// dynamic shared memory of the fused kernel.
+cudaError_t launch_fused_need(const Space &sp, const SpaceTables &tb, int *need, cudaStream_t st);
+cudaError_t fused_config(const Space &sp, int *grid, size_t *smem);
 
 // One member of a batched Lanczos, as the batched H.psi kernels see it
 // (momentum-block pair matrix only).

@@ -31,7 +31,7 @@ struct DevPairOp {
     PairOp view() const
     {
         return PairOp{rowptr, col, val, hdiag, hfull, nnz, hblk, nhblk, create_form, status, hdense,
-                      wait_cycles, test_stall, hblk_h.empty() ? nullptr : hblk_h.data()};
+                      wait_cycles, test_stall, hblk_h.empty() ? nullptr : hblk_h.data(), FusedPlan{}};
     }
     BlockOp blocks() const { return BlockOp{prog, prog_bytes}; }
 };
@@ -68,6 +68,12 @@ struct mcpi_space_s {
     int test_stall = 0;              // MCPI_OPT_TEST_STALL_GATHER
     bool no_occ = false;             // MCPI_OPT_NO_OCC_TABLES
     int create_form = 0;            // pair-creation kernel form (MCPI_OPT_CREATE_FORM)
+    // fused H.psi (MCPI_OPT_FUSED_*): schedule built once per space by ensure_fused
+    bool fused_on = false;
+    int fused_lead = 128;
+    bool fz_ready = false;
+    mcpi::FusedPlan fz{};
+    int *d_fz = nullptr;             // one allocation: need | order | flags | ctl
     // grow-only workspaces kept between calls: Krylov basis of mcpi_ground,
     // state block and residual of mcpi_lanczos
     void *d_basis = nullptr, *d_lzblk = nullptr, *d_lzr = nullptr;
