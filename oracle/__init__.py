@@ -118,6 +118,8 @@ class Orc:
                                   _vp, _vp, _vp, _vp, ct.c_int64, ct.c_int64, ct.c_int]
         L.orc_obrho.argtypes = [ct.c_int, ct.c_int, _vp, _vp, _vp, _vp]
         L.orc_density_generic.argtypes = [ct.c_int, ct.c_int, ct.c_int, _vp, _vp, _vp]
+        L.orc_density_rows.argtypes = [ct.c_int, ct.c_int, ct.c_int, _vp, _vp, _vp, ct.c_int64,
+                                       ct.c_int64, ct.c_int]
         L.orc_apply_h_generic.argtypes = [ct.c_int, ct.c_int, _vp, _vp, _vp, _vp]
         L.orc_lieb_ho.argtypes = [ct.c_int, ct.c_double, _vp]
         L.orc_lieb_hint.argtypes = [ct.c_int, ct.c_double, _vp]
@@ -208,6 +210,15 @@ class Orc:
         t = np.zeros(M ** (2 * order), np.complex128)
         self.lib.orc_density_generic(N, M, order, _ptr(np.ascontiguousarray(phi)),
                                      _ptr(np.ascontiguousarray(psi)), _ptr(t))
+        return t
+
+    def density_rows(self, N, M, order, phi, psi, row0, row1, threads=0):
+        """density() with the ket restricted to rows [row0, row1): <phi| ... |psi_S>."""
+        t = np.zeros(M ** (2 * order), np.complex128)
+        rc = self.lib.orc_density_rows(N, M, order, _ptr(np.ascontiguousarray(phi)),
+                                       _ptr(np.ascontiguousarray(psi)), _ptr(t), int(row0), int(row1),
+                                       threads or os.cpu_count())
+        assert rc == 0
         return t
 
     def apply_h_generic(self, N, M, Ho, Hint, psi):

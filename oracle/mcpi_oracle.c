@@ -16,7 +16,7 @@
  *   orc_apply_h                  hamiltonianMatrix.h:31-425 (plain), :431-887 (_X),
  *                                :891-1425 (_XX), :1431-1970 (_omp = _XX over threads)
  *   orc_obrho                    onebodyMatrix.h:190-251      OBrho_XM
- *   orc_density_generic          definition of rho1/rho2 in onebodyMatrix.h:20-30 and
+ *   orc_density_generic / _rows  definition of rho1/rho2 in onebodyMatrix.h:20-30 and
  *                                twobodyMatrix.h:20-36, evaluated term by term for a
  *                                bra/ket pair (also gives the transition densities)
  *   orc_apply_h_generic          H = sum Ho a+a + 1/2 sum Hint a+a+aa, unfolded
@@ -615,17 +615,19 @@ int orc_obrho(int N, int M, const int32_t *IF, const int32_t *Map, const zc *C, 
  *   t2[k + s*M + q*M^2 + l*M^3] = <phi| a+_k a+_s a_q a_l |psi>  (order 2)
  * (index conventions of onebodyMatrix.h / twobodyMatrix.h; with phi = psi
  * these are rho1 and rho2). Every entry is reduced: no symmetry fill, so the
- * result is valid when phi != psi. Cost nc*M^4*O(M): small cases only. */
-int orc_density_generic(int N, int M, int order, const zc *phi, const zc *psi, zc *t)
+ * result is valid when phi != psi. Only ket rows i in [row0, row1) are summed
+ * (the whole space: 0, nc), i.e. the result is <phi| ... |psi_S> with psi_S
+ * the ket restricted to those rows. Cost (row1-row0)*M^4*O(M). Rows are
+ * split into nthreads fixed chunks whose partial sums are added in chunk
+ * order. */
+static void density_rows(const space_t *sp, int order, const zc *phi, const zc *psi, zc *t, int64_t r0,
+                         int64_t r1)
 {
-    space_t sp;
-    if (M > 64 || space_init(&sp, N, M)) return -1;
-    int64_t nc = sp.nc, M2 = (int64_t)M * M, M3 = M2 * M;
-    int64_t nout = order == 1 ? M2 : M2 * M2;
-    for (int64_t x = 0; x < nout; x++) t[x] = 0;
+    int M = sp->M;
+    int64_t M2 = (int64_t)M * M, M3 = M2 * M;
     int v[64];
-    for (int64_t i = 0; i < nc; i++) {
-        index_to_fock(&sp, i, v);
+    for (int64_t i = r0; i < r1; i++) {
+        index_to_fock(sp, i, v);
         if (order == 1) {
             for (int l = 0; l < M; l++) {
                 if (v[l] < 1) continue;
@@ -634,7 +636,7 @@ int orc_density_generic(int N, int M, int order, const zc *phi, const zc *psi, z
                 for (int k = 0; k < M; k++) {
                     double f = f1 * sqrt((double)(v[k] + 1));
                     v[k]++;
-                    int64_t j = fock_to_index(&sp, v);
+                    int64_t j = fock_to_index(sp, v);
                     v[k]--;
                     t[k + l * M] += conj(phi[j]) * psi[i] * f;
                 }
@@ -655,10 +657,9 @@ int orc_density_generic(int N, int M, int order, const zc *phi, const zc *psi, z
                         for (int k = 0; k < M; k++) {
                             double fk = sqrt((double)(v[k] + 1));
                             v[k]++;
-                            int64_t j = fock_to_index(&sp, v);
+                            int64_t j = fock_to_index(sp, v);
                             v[k]--;
-                            t[k + s * M + q * M2 + l * M3] +=
-                                conj(phi[j]) * psi[i] * (fl * fq * fs * fk);
+                            t[k + s * M + q * M2 + l * M3] += conj(phi[j]) * psi[i] * (fl * fq * fs * fk);
                         }
                         v[s]--;
                     }
@@ -668,6 +669,48 @@ int orc_density_generic(int N, int M, int order, const zc *phi, const zc *psi, z
             }
         }
     }
+}
+
+int orc_density_rows(int N, int M, int order, const zc *phi, const zc *psi, zc *t, int64_t row0, int64_t row1,
+                     int nthreads)
+{
+    space_t sp;
+    if (M > 64 || space_init(&sp, N, M)) return -1;
+    if (row0 < 0 || row1 > sp.nc || row0 > row1) {
+        space_free(&sp);
+        return -1;
+    }
+    int64_t M2 = (int64_t)M * M;
+    int64_t nout = order == 1 ? M2 : M2 * M2;
+    if (nthreads < 1) nthreads = 1;
+    zc *part = (zc *)calloc((size_t)nthreads * nout, sizeof(zc));
+    if (!part) {
+        space_free(&sp);
+        return -1;
+    }
+    int64_t n = row1 - row0;
+#pragma omp parallel for schedule(static, 1) num_threads(nthreads)
+    for (int c = 0; c < nthreads; c++)
+        density_rows(&sp, order, phi, psi, part + (int64_t)c * nout, row0 + n * c / nthreads,
+                     row0 + n * (c + 1) / nthreads);
+    for (int64_t x = 0; x < nout; x++) {
+        zc z = 0;
+        for (int c = 0; c < nthreads; c++) z += part[(int64_t)c * nout + x];
+        t[x] = z;
+    }
+    free(part);
+    space_free(&sp);
+    return 0;
+}
+
+int orc_density_generic(int N, int M, int order, const zc *phi, const zc *psi, zc *t)
+{
+    space_t sp;
+    if (M > 64 || space_init(&sp, N, M)) return -1;
+    int64_t M2 = (int64_t)M * M;
+    int64_t nout = order == 1 ? M2 : M2 * M2;
+    for (int64_t x = 0; x < nout; x++) t[x] = 0;
+    density_rows(&sp, order, phi, psi, t, 0, sp.nc);
     space_free(&sp);
     return 0;
 }

@@ -142,8 +142,7 @@ def test_densities_oracle(orc, N, M):
     assert rel(r1, orc.obrho(N, M, C)) <= TOL
     assert abs(np.trace(r1) - N) <= 1e-12 * max(N, 1)
     r2 = sp.rho2(C).cpu().numpy()
-    if N * M ** 4 * orc.nc(N, M) <= 2e9:
-        assert rel(r2, orc.density(N, M, 2, C, C)) <= TOL
+    assert rel(r2, orc.density_rows(N, M, 2, C, C, 0, orc.nc(N, M))) <= TOL
     R = r2.reshape(M, M, M, M)          # axes (l, q, s, k)
     tr = sum(R[k, s, s, k] for k in range(M) for s in range(M))   # sum <a+_k a+_s a_s a_k>
     assert abs(tr - N * (N - 1)) <= 1e-12 * max(1, N * N)

@@ -5,11 +5,13 @@ compiled unmodified) are always checked; where oracle/_ref/libmcpi_ref.so is
 present the restatement is also compared live against the reference.
 No GPU needed.
 """
+import os
+
 import numpy as np
 import pytest
 
 import oracle
-from conftest import case_keys, rel
+from conftest import GOLDEN, case_keys, rel
 
 TABLE_NAMES = ["NCmat", "IF", "Map", "MapOT", "strideOT", "MapTT", "strideTT"]
 
@@ -135,3 +137,50 @@ def test_restatement_against_live_reference(orc):
         assert np.array_equal(orc.apply_h(N, M, C, Ho, Hint, mode=0), R.apply_h("plain", N, M, C, Ho, Hint, t))
         assert np.array_equal(orc.apply_h(N, M, C, Ho, Hint, mode=2),
                               R.apply_h("omp", N, M, C, Ho, Hint, t))
+
+
+def test_density_rows_add_up(orc):
+    # the ket row ranges of orc_density_rows partition the full definition
+    N, M = 5, 6
+    rng = np.random.default_rng(3)
+    nc = orc.nc(N, M)
+    phi = rng.standard_normal(nc) + 1j * rng.standard_normal(nc)
+    psi = rng.standard_normal(nc) + 1j * rng.standard_normal(nc)
+    for order in (1, 2):
+        full = orc.density(N, M, order, phi, psi)
+        parts = orc.density_rows(N, M, order, phi, psi, 0, 97) + orc.density_rows(N, M, order, phi, psi, 97, nc)
+        assert np.abs(full - parts).max() <= 1e-13 * np.abs(full).max()
+        cut = psi.copy()
+        cut[97:] = 0
+        assert np.abs(orc.density(N, M, order, phi, cut) - orc.density_rows(N, M, order, phi, psi, 0, 97)).max() \
+            <= 1e-13 * np.abs(full).max()
+
+
+def test_c0_density_fixture_against_oracle(orc):
+    # the reference's TBrho_XX / OBrho_XM at N=10, M=10 (tests/golden/c0_densities.npz)
+    # against the oracle's own restatements
+    f = np.load(os.path.join(GOLDEN, "c0_densities.npz"))
+    N, M = int(f["N"]), int(f["M"])
+    C = oracle.random_inputs(N, M, int(f["seed"]))[0]
+    assert np.array_equal(C[:8], f["C_head"]) and C.sum() == f["C_sum"]
+    assert np.abs(orc.obrho(N, M, C) - f["rho1"]).max() <= 1e-13
+    r2 = orc.density_rows(N, M, 2, C, C, 0, orc.nc(N, M))
+    assert np.linalg.norm(r2 - f["rho2"]) <= 1e-12 * np.linalg.norm(f["rho2"])
+
+
+def test_lanczos_fixtures_are_consistent():
+    # the configuration-size fixtures' own arithmetic: E0 is the lowest Ritz
+    # value of the stored tridiagonal, occupations add up to N, and the sweep
+    # members are the draw the batched benchmark makes
+    from scipy.linalg import eigh_tridiagonal
+    f = np.load(os.path.join(GOLDEN, "lanczos_c1.npz"))
+    w = eigh_tridiagonal(f["alpha"], f["beta"], eigvals_only=True)
+    assert abs(w[0] - f["E0"]) <= 1e-12 * abs(f["E0"])
+    assert abs(f["occupations"].sum() - f["N"]) <= 1e-10
+    s = np.load(os.path.join(GOLDEN, "sweep_c2.npz"))
+    rng = np.random.default_rng(2024)
+    n = rng.integers(6, 15, 64)
+    m = rng.choice([7, 9, 11], 64)
+    g = 10.0 ** rng.uniform(-2.0, 2.0, 64)
+    assert np.array_equal(s["N"], n) and np.array_equal(s["M"], m) and np.array_equal(s["g"], g)
+    assert len(s["pick"]) == len(s["E0"]) >= 4
