@@ -80,9 +80,10 @@ MCPI_API int mcpi_space_sync(mcpi_space sp);
  * default: about two seconds). A wait that runs out makes the kernel return
  * and the next synchronising call report MCPI_ERR_TIMEOUT. */
 #define MCPI_OPT_WAIT_LIMIT_KCYCLES 5
-/* MCPI_OPT_TEST_STALL_GATHER (0/1): for testing the timeout path only — the
- * dense-product kernel's gather warps deliver no tile, so its product warps'
- * waits run out (results are invalid while it is set). */
+/* MCPI_OPT_TEST_STALL_GATHER (0/1): for testing the timeout paths only — the
+ * gather warps of the dense-product and tensor-core Gram kernels deliver no
+ * tile and the fused H.psi kernel's producers never count themselves done, so
+ * the waits run out (results are invalid while it is set). */
 #define MCPI_OPT_TEST_STALL_GATHER 6
 /* MCPI_OPT_NO_OCC_TABLES (0/1): build no packed occupation tables (the H.psi
  * kernels then decode every row index; 1 also frees existing tables). Takes

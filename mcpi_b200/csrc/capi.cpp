@@ -932,7 +932,8 @@ static int density(mcpi_space sp, int order, const void *phi, const void *psi, v
     int rc = ensure_gram(sp);
     if (rc) return rc;
     CK(mcpi::launch_density(sp->sp, sp->tables(), order, (const double2 *)phi, (const double2 *)psi,
-                            sp->d_gram, (double2 *)out, sp->stream));
+                            sp->d_gram, (double2 *)out, sp->stream, sp->d_status, sp->wait_cycles,
+                            sp->test_stall));
     return MCPI_OK;
 }
 

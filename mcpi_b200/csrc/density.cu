@@ -21,6 +21,7 @@
 #include <cuda_runtime.h>
 #include "fock.cuh"
 #include "kernels.h"
+#include "mbarrier.cuh"
 
 namespace mcpi {
 
@@ -29,6 +30,7 @@ namespace {
 constexpr int kTile = 32;       // hole configurations per tile
 constexpr int kThreads = 256;
 constexpr int kGramBlocks = 296;  // 2 x 148 SMs
+constexpr int kDmmaBlocks = 148;  // one persistent block per SM (fixed: it sets the reduction order)
 
 __device__ __forceinline__ void cfma_conj(double2 &acc, double2 a, double2 b)
 {
@@ -183,6 +185,255 @@ __global__ void __launch_bounds__(kThreads) k_gram(Space sp, SpaceTables tb,
     }
 }
 
+// ---------------------------------------------------------------------------
+// rho2 and the transition rho2 on the FP64 tensor cores (M <= 12).
+// G[a][b] = sum_m conj(Dphi[a][m]) Dpsi[b][m] is a K x K product reduced over
+// the (N-2) space, K = M(M+1)/2: with mma.sync.m16n8k4.f64 the rows are pairs
+// a (16 per MMA), the columns pairs b (8 per MMA) and the reduction runs over
+// configurations m (4 per MMA). The complex product takes three real ones
+// (Gauss): t1 += Ar Br, t2 += Ai Bi, t3 += (Ar - Ai)(Br + Bi), and at the end
+// Re G = t1 + t2, Im G = t3 - t1 + t2 (A = Dphi, conjugated by the signs).
+// One persistent block per SM, warp-specialised: 8 gather warps fill tiles of
+// GM configurations (one decode per configuration, K scattered 16-byte loads
+// of each vector from L2, the factors c_b(m), real and imaginary parts into
+// separate row-major planes) into two stages; 8 product warps each own a
+// fixed set of 16 x 8 output tiles and keep their accumulators in registers
+// across all of the block's configuration tiles. With one state the Gram
+// matrix is Hermitian: only the tiles (i, j) with j >= 2i are reduced (16 of
+// 28 at M = 10) and the finish kernel takes the others as conjugates of their
+// mirror entries. Hand-over by mbarriers whose waits are bounded (about two
+// seconds; then the status word reports MCPI_ERR_TIMEOUT). Per-block partials
+// are summed in block order by k_gram_finish: deterministic.
+// Plane layout: row r (pair) at r * LD doubles, LD = GM + 4, so the 8 rows x 4
+// consecutive configurations of one fragment load fall into distinct banks.
+// ---------------------------------------------------------------------------
+constexpr int kDmmaPW = 8;                            // product warps
+constexpr int kDmmaGW = 8;                            // gather warps
+constexpr int kDmmaThreads = (kDmmaPW + kDmmaGW) * 32;
+constexpr int kDmmaStages = 2;
+constexpr int kDmmaUnroll = 4;   // configuration steps of the product loop unrolled together
+constexpr int kDmmaMaxM = 12;        // rho2 of one state
+constexpr int kDmmaMaxMTrans = 10;   // transition rho2 (more accumulators: larger M would spill)
+
+template <int M, bool SAME>
+struct DmmaGram {
+    static constexpr int K = M * (M + 1) / 2;
+    static constexpr int AG = (K + 15) / 16;         // 16-row groups of a
+    static constexpr int BG = (K + 7) / 8;           // 8-column groups of b
+    static constexpr int KP = AG * 16;               // padded plane rows (>= BG * 8)
+    // SUMS: the gather warps form the Gauss sum planes Ar - Ai and Br + Bi
+    // (the transition form: measured 4.45 against 4.70 ms at N=20, M=10);
+    // otherwise the product warps add the fragments themselves (one state:
+    // half the planes, so tiles of 64 configurations fit two stages -- with
+    // sum planes and 32-configuration tiles it took 4.6 against 2.9 ms).
+    static constexpr bool SUMS = !SAME;
+    static constexpr int NP = SAME ? 2 : 6;
+    static constexpr int GM = SAME ? 64 : 32;        // configurations per tile
+    static constexpr int LD = GM + 4;                // plane row stride (doubles)
+    static constexpr int GT = kDmmaGW * 32;          // gather threads
+    static constexpr int PARTS = GT / GM;            // gather threads per configuration
+    static constexpr int ntiles()
+    {
+        int n = 0;
+        for (int i = 0; i < AG; ++i)
+            for (int j = 0; j < BG; ++j)
+                if (!SAME || j >= 2 * i) ++n;
+        return n;
+    }
+    static constexpr int NT = ntiles();
+    static constexpr int TPW = (NT + kDmmaPW - 1) / kDmmaPW;   // tiles per product warp
+    static constexpr size_t stage_bytes = sizeof(double) * NP * KP * LD;
+    // planes, then the stage barriers, then the space's sqrt and binomial tables
+    static size_t smem(int ws)
+    {
+        return kDmmaStages * stage_bytes + 2 * kDmmaStages * sizeof(uint64_t) + sizeof(double) * ws +
+               sizeof(uint32_t) * (M - 1) * ws;
+    }
+};
+
+// Output tile n (in i-major order over the kept tiles) -> (i, j).
+template <int M, bool SAME>
+__device__ __forceinline__ void dmma_tile(int n, int &i, int &j)
+{
+    using D = DmmaGram<M, SAME>;
+    i = 0;
+    j = 0;
+    for (int a = 0; a < D::AG; ++a) {
+        const int j0 = SAME ? 2 * a : 0;
+        const int cnt = D::BG > j0 ? D::BG - j0 : 0;
+        if (n < cnt) {
+            i = a;
+            j = j0 + n;
+            return;
+        }
+        n -= cnt;
+    }
+}
+
+__device__ __forceinline__ void dmma_m16n8k4(double (&c)[4], double a0, double a1, double b)
+{
+    asm("mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0, %1, %2, %3}, {%4, %5}, {%6}, {%0, %1, %2, %3};\n"
+        : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+        : "d"(a0), "d"(a1), "d"(b));
+}
+
+template <int M, bool SAME>
+__global__ void __launch_bounds__(kDmmaThreads, 1)
+    k_gram_dmma(Space sp, SpaceTables tb, const double2 *__restrict__ phi, const double2 *__restrict__ psi,
+                double2 *__restrict__ partial, int *status, long long wait_cycles, int test_stall)
+{
+    using D = DmmaGram<M, SAME>;
+    constexpr int K = D::K, KP = D::KP, LD = D::LD, GM = D::GM;
+    const long long limit = wait_cycles > 0 ? wait_cycles : kWaitCycles;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double *planes = reinterpret_cast<double *>(smem_raw);                    // stages x NP x KP x LD
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem_raw + kDmmaStages * D::stage_bytes);
+    uint64_t *empty = full + kDmmaStages;
+    double *sq = reinterpret_cast<double *>(empty + kDmmaStages);          // wstride
+    uint32_t *W = reinterpret_cast<uint32_t *>(sq + sp.wstride);          // (M-1) x wstride
+    const int ws = sp.wstride;
+    for (int x = threadIdx.x; x < (M - 1) * ws; x += blockDim.x) W[x] = tb.W[x];
+    for (int x = threadIdx.x; x < ws; x += blockDim.x) sq[x] = tb.sq[x];
+    // padding rows K .. KP-1 of every plane stay zero
+    for (int x = threadIdx.x; x < kDmmaStages * D::NP * (KP - K) * LD; x += blockDim.x) {
+        const int per = (KP - K) * LD, pl = x / per, r = x % per;
+        planes[(size_t)pl * KP * LD + K * LD + r] = 0.0;
+    }
+    if (threadIdx.x == 0)
+        for (int b = 0; b < kDmmaStages; ++b) {
+            mbar_init(full + b, D::GT);
+            mbar_init(empty + b, kDmmaPW);
+        }
+    __syncthreads();
+
+    const uint32_t nh = sp.nc2;
+    const uint32_t ntiles = (nh + GM - 1) / GM;
+    const uint32_t ntb = blockIdx.x < ntiles ? (ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x : 0;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    if (warp >= kDmmaPW) {
+        // gather: configuration ml of the tile, pair columns col % PARTS == part
+        const int g = threadIdx.x - kDmmaPW * 32;
+        const int ml = g % GM, part = g / GM;
+        for (uint32_t it = 0; it < ntb; ++it) {
+            const int st = it % kDmmaStages;
+            if (test_stall) return;   // test switch: deliver nothing, so that the product warps' waits run out
+            if (it >= kDmmaStages && !mbar_wait(empty + st, (it / kDmmaStages - 1) & 1, limit)) {
+                if (status) atomicExch(status, 1);
+                return;
+            }
+            double *pl = planes + (size_t)st * D::NP * KP * LD;
+            const uint32_t m = (blockIdx.x + it * gridDim.x) * GM + ml;
+            if (m < nh) {
+                int u[M], Q[M];
+                occupations<M>(tb.occ2, tb.occ_bits, m, sp.N - 2, nh, W, ws, u, Q);
+                uint32_t B0[M], B1[M], B2[M];
+                prefix_table<M>(Q, 0, W, ws, B0);
+                prefix_table<M>(Q, 1, W, ws, B1);
+                prefix_table<M>(Q, 2, W, ws, B2);
+#pragma unroll
+                for (int q = 0; q < M; ++q)
+#pragma unroll
+                    for (int l = q; l < M; ++l) {
+                        const int col = pair_index(q, l, M);
+                        if (col % D::PARTS != part) continue;
+                        const uint32_t j = idx_add2(sp.nc, B0, B1, B2, q, l, M);
+                        const double c = (q == l) ? sq[u[q] + 1] * sq[u[q] + 2] : sq[u[q] + 1] * sq[u[l] + 1];
+                        const double2 x = __ldg(phi + j);
+                        const double xr = c * x.x, xi = c * x.y;
+                        pl[col * LD + ml] = xr;
+                        pl[(KP + col) * LD + ml] = xi;
+                        if constexpr (D::SUMS) {
+                            const double2 y = __ldg(psi + j);
+                            const double yr = c * y.x, yi = c * y.y;
+                            pl[(2 * KP + col) * LD + ml] = xr - xi;
+                            pl[(3 * KP + col) * LD + ml] = yr;
+                            pl[(4 * KP + col) * LD + ml] = yi;
+                            pl[(5 * KP + col) * LD + ml] = yr + yi;
+                        }
+                    }
+            } else {
+                for (int col = part; col < K; col += D::PARTS)
+#pragma unroll
+                    for (int p = 0; p < D::NP; ++p) pl[(p * KP + col) * LD + ml] = 0.0;
+            }
+            mbar_arrive(full + st);
+        }
+        return;
+    }
+
+    // product warps: tiles n = warp * TPW + x
+    const int gq = lane >> 2, tq = lane & 3;
+    double acc[D::TPW][3][4];
+#pragma unroll
+    for (int x = 0; x < D::TPW; ++x)
+#pragma unroll
+        for (int y = 0; y < 3; ++y)
+#pragma unroll
+            for (int z = 0; z < 4; ++z) acc[x][y][z] = 0.0;
+    int ti[D::TPW], tj[D::TPW];
+#pragma unroll
+    for (int x = 0; x < D::TPW; ++x) dmma_tile<M, SAME>(warp * D::TPW + x, ti[x], tj[x]);
+    for (uint32_t it = 0; it < ntb; ++it) {
+        const int st = it % kDmmaStages;
+        if (!mbar_wait(full + st, (it / kDmmaStages) & 1, limit)) {
+            if (lane == 0 && status) atomicExch(status, 1);
+            return;
+        }
+        const double *Ar = planes + (size_t)st * D::NP * KP * LD;
+        const double *Ai = Ar + KP * LD;
+        const double *As = Ar + 2 * KP * LD;                                      // SUMS only
+        const double *Br = SAME ? Ar : Ar + 3 * KP * LD;
+        const double *Bi = SAME ? Ai : Ar + 4 * KP * LD;
+        const double *Bs = Ar + 5 * KP * LD;                                      // SUMS only
+#pragma unroll kDmmaUnroll
+        for (int s = 0; s < GM / 4; ++s) {
+            const int cm = 4 * s + tq;
+            int icur = -1;
+            double ar0 = 0, ar1 = 0, ai0 = 0, ai1 = 0, as0 = 0, as1 = 0;
+#pragma unroll
+            for (int x = 0; x < D::TPW; ++x) {
+                if (warp * D::TPW + x >= D::NT) break;
+                if (ti[x] != icur) {   // warp-uniform: reload A only for a new row group
+                    icur = ti[x];
+                    const int r0 = (16 * icur + gq) * LD + cm, r1 = r0 + 8 * LD;
+                    ar0 = Ar[r0];
+                    ar1 = Ar[r1];
+                    ai0 = Ai[r0];
+                    ai1 = Ai[r1];
+                    if constexpr (D::SUMS) {
+                        as0 = As[r0];
+                        as1 = As[r1];
+                    } else {
+                        as0 = ar0 - ai0;
+                        as1 = ar1 - ai1;
+                    }
+                }
+                const int rb = (8 * tj[x] + gq) * LD + cm;
+                const double br = Br[rb], bi = Bi[rb];
+                dmma_m16n8k4(acc[x][0], ar0, ar1, br);
+                dmma_m16n8k4(acc[x][1], ai0, ai1, bi);
+                dmma_m16n8k4(acc[x][2], as0, as1, D::SUMS ? Bs[rb] : br + bi);
+            }
+        }
+        __syncwarp();
+        if (lane == 0 && it + kDmmaStages < ntb) mbar_arrive(empty + st);
+    }
+    double2 *out = partial + (size_t)blockIdx.x * K * K;
+#pragma unroll
+    for (int x = 0; x < D::TPW; ++x) {
+        if (warp * D::TPW + x >= D::NT) break;
+#pragma unroll
+        for (int z = 0; z < 4; ++z) {
+            const int a = 16 * ti[x] + gq + (z >= 2 ? 8 : 0), b = 8 * tj[x] + 2 * tq + (z & 1);
+            if (a < K && b < K) {
+                const double t1 = acc[x][0][z], t2 = acc[x][1][z], t3 = acc[x][2][z];
+                out[a * K + b] = make_double2(t1 + t2, t3 - t1 + t2);
+            }
+        }
+    }
+}
+
 // rho1 (and the transition rho1): G[a][b] = sum_h conj(Dphi[a][h]) Dpsi[b][h] over
 // the N-1 space with D[l][h] = sqrt(u_l+1) x[index(h + e_l)]. Only M columns, so
 // the Gram kernel above would keep one 4x4 block per thread busy (9 threads of
@@ -280,9 +531,11 @@ __global__ void __launch_bounds__(kThreads) k_rho1(Space sp, SpaceTables tb, con
 }
 
 // Sums the per-CTA partials in block order and writes the reference layout.
-// HERM: the partials hold only the blocks of k_gram<.., SAME = true> (entry
-// (a, b) with a mod NB <= b mod NB); the rest is conj of the entry (b, a).
-template <int M, int ORDER, bool HERM = false>
+// HERM 1: the partials hold only the blocks of k_gram<.., SAME = true> (entry
+// (a, b) with a mod NB <= b mod NB); HERM 2: only the tiles of
+// k_gram_dmma<.., SAME = true> (entry (a, b) with b / 8 >= 2 (a / 16)). The
+// rest is the conjugate of the entry (b, a), which is then held.
+template <int M, int ORDER, int HERM = 0>
 __global__ void k_gram_finish(const double2 *__restrict__ partial, int nblocks,
                               double2 *__restrict__ out)
 {
@@ -299,7 +552,7 @@ __global__ void k_gram_finish(const double2 *__restrict__ partial, int nblocks,
         a = k <= s ? pair_index(k, s, M) : pair_index(s, k, M);
         b = q <= l ? pair_index(q, l, M) : pair_index(l, q, M);
     }
-    const bool mirror = HERM && (a % C::NB) > (b % C::NB);
+    const bool mirror = HERM == 1 ? (a % C::NB) > (b % C::NB) : HERM == 2 ? (b / 8) < 2 * (a / 16) : false;
     const int e = mirror ? b * C::K + a : a * C::K + b;
     double2 acc = make_double2(0.0, 0.0);
     for (int blk = 0; blk < nblocks; ++blk) {
@@ -313,7 +566,8 @@ __global__ void k_gram_finish(const double2 *__restrict__ partial, int nblocks,
 
 template <int M, int ORDER>
 cudaError_t density_m(const Space &sp, const SpaceTables &tb, const double2 *phi,
-                      const double2 *psi, double2 *partial, double2 *out, cudaStream_t st)
+                      const double2 *psi, double2 *partial, double2 *out, cudaStream_t st, int *status,
+                      long long wait_cycles, int test_stall)
 {
     using C = Cols<M, ORDER>;
     const bool same = (phi == psi);
@@ -335,6 +589,41 @@ cudaError_t density_m(const Space &sp, const SpaceTables &tb, const double2 *phi
         k_gram_finish<M, 1><<<(M * M + 255) / 256, 256, 0, st>>>(partial, gx, out);
         return cudaGetLastError();
     }
+    if constexpr (ORDER == 2 && M >= 2 && M <= kDmmaMaxM) {
+        // FP64 tensor cores (the transition form up to kDmmaMaxMTrans), when the
+        // stages and the space's tables fit the block's shared memory
+        const int nout = M * M * M * M;
+        int dev = 0, optin = 0;
+        cudaError_t qe = cudaGetDevice(&dev);
+        if (qe == cudaSuccess) qe = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        if (qe != cudaSuccess) return qe;
+        if (same && DmmaGram<M, true>::smem(sp.wstride) <= (size_t)optin) {
+            using Dm = DmmaGram<M, true>;
+            const unsigned ntiles = (sp.nc2 + Dm::GM - 1) / Dm::GM;
+            const unsigned gx = ntiles < (unsigned)kDmmaBlocks ? (ntiles ? ntiles : 1) : kDmmaBlocks;
+            const size_t sm = Dm::smem(sp.wstride);
+            cudaError_t e = cudaFuncSetAttribute(k_gram_dmma<M, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+            if (e != cudaSuccess) return e;
+            k_gram_dmma<M, true><<<gx, kDmmaThreads, sm, st>>>(sp, tb, phi, psi, partial, status, wait_cycles,
+                                                               test_stall);
+            k_gram_finish<M, 2, 2><<<(nout + 255) / 256, 256, 0, st>>>(partial, gx, out);
+            return cudaGetLastError();
+        }
+        if constexpr (M <= kDmmaMaxMTrans) {
+            if (!same && DmmaGram<M, false>::smem(sp.wstride) <= (size_t)optin) {
+            using Dm = DmmaGram<M, false>;
+            const unsigned ntiles = (sp.nc2 + Dm::GM - 1) / Dm::GM;
+            const unsigned gx = ntiles < (unsigned)kDmmaBlocks ? (ntiles ? ntiles : 1) : kDmmaBlocks;
+            const size_t sm = Dm::smem(sp.wstride);
+            cudaError_t e = cudaFuncSetAttribute(k_gram_dmma<M, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+            if (e != cudaSuccess) return e;
+            k_gram_dmma<M, false><<<gx, kDmmaThreads, sm, st>>>(sp, tb, phi, psi, partial, status, wait_cycles,
+                                                                test_stall);
+            k_gram_finish<M, 2, 0><<<(nout + 255) / 256, 256, 0, st>>>(partial, gx, out);
+            return cudaGetLastError();
+            }
+        }
+    }
     const size_t tiles = sizeof(double2) * C::KP * C::LD * (same ? 1 : 2);
     const size_t smem = tiles + sizeof(double) * sp.wstride + sizeof(uint32_t) * (M - 1) * sp.wstride;
     const uint32_t nh = ORDER == 2 ? sp.nc2 : sp.nc1;
@@ -355,9 +644,9 @@ cudaError_t density_m(const Space &sp, const SpaceTables &tb, const double2 *phi
     }
     const int nout = ORDER == 1 ? M * M : M * M * M * M;
     if (same)
-        k_gram_finish<M, ORDER, true><<<(nout + 255) / 256, 256, 0, st>>>(partial, gx, out);
+        k_gram_finish<M, ORDER, 1><<<(nout + 255) / 256, 256, 0, st>>>(partial, gx, out);
     else
-        k_gram_finish<M, ORDER, false><<<(nout + 255) / 256, 256, 0, st>>>(partial, gx, out);
+        k_gram_finish<M, ORDER, 0><<<(nout + 255) / 256, 256, 0, st>>>(partial, gx, out);
     return cudaGetLastError();
 }
 
@@ -370,14 +659,15 @@ size_t gram_partial_elems(const Space &sp, int order)
 }
 
 cudaError_t launch_density(const Space &sp, const SpaceTables &tb, int order, const double2 *phi,
-                           const double2 *psi, double2 *partial, double2 *out, cudaStream_t st)
+                           const double2 *psi, double2 *partial, double2 *out, cudaStream_t st, int *status,
+                           long long wait_cycles, int test_stall)
 {
     const int nout = order == 1 ? sp.M * sp.M : sp.M * sp.M * sp.M * sp.M;
     if (sp.N < order) return cudaMemsetAsync(out, 0, sizeof(double2) * nout, st);
     switch (sp.M * 4 + order) {
 #define MCPI_CASE(m)                                                                      \
-    case m * 4 + 1: return density_m<m, 1>(sp, tb, phi, psi, partial, out, st);          \
-    case m * 4 + 2: return density_m<m, 2>(sp, tb, phi, psi, partial, out, st);
+    case m * 4 + 1: return density_m<m, 1>(sp, tb, phi, psi, partial, out, st, status, wait_cycles, test_stall); \
+    case m * 4 + 2: return density_m<m, 2>(sp, tb, phi, psi, partial, out, st, status, wait_cycles, test_stall);
         MCPI_CASE(1) MCPI_CASE(2) MCPI_CASE(3) MCPI_CASE(4) MCPI_CASE(5) MCPI_CASE(6)
         MCPI_CASE(7) MCPI_CASE(8) MCPI_CASE(9) MCPI_CASE(10) MCPI_CASE(11) MCPI_CASE(12)
         MCPI_CASE(13) MCPI_CASE(14) MCPI_CASE(15) MCPI_CASE(16)

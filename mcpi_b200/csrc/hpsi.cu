@@ -25,6 +25,7 @@
 #include <cuda_runtime.h>
 #include "fock.cuh"
 #include "kernels.h"
+#include "mbarrier.cuh"
 
 namespace mcpi {
 
@@ -404,43 +405,6 @@ __global__ void __launch_bounds__(kTG, M <= 10 ? 2 : 1)
 // (with no copies of its own in flight), so a stuck pipeline ends the kernel
 // with an error instead of hanging.
 constexpr int kTW = 2 * kTG + 2 * kGM;   // threads per block, warp-specialised form
-constexpr long long kWaitCycles = 4000000000LL;
-
-__device__ __forceinline__ uint32_t smem_addr(const void *p)
-{
-    return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
-{
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_addr(bar)) : "memory");
-}
-
-// true once the phase of the given parity has completed; false after limit cycles
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long long limit)
-{
-    const long long t0 = clock64();
-    for (;;) {
-        uint32_t ok;
-        asm volatile(
-            "{\n"
-            ".reg .pred p;\n"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-            "selp.u32 %0, 1, 0, p;\n"
-            "}\n"
-            : "=r"(ok)
-            : "r"(smem_addr(bar)), "r"(parity)
-            : "memory");
-        if (ok) return true;
-        if (clock64() - t0 > limit) return false;
-    }
-}
-
 template <int M, int NS, bool CS>
 __global__ void __launch_bounds__(kTW, 1)
     k_pair_annihilate_gemm_ws(Space sp, SpaceTables tb, const double2 *__restrict__ H,

@@ -143,9 +143,13 @@ int batch_rows_per_block(int stage);
 // layouts: order 1 -> rho1[k*M + l]; order 2 -> rho2[k + s*M + q*M^2 + l*M^3].
 // partial: scratch of >= gram_partial_elems(sp, order) complex.
 size_t gram_partial_elems(const Space &sp, int order);
+// status / wait_cycles: the space's status word and the limit of the bounded
+// waits of the tensor-core Gram kernel (0: about two seconds); test_stall
+// keeps its gather warps from delivering any tile (testing the timeout path).
 cudaError_t launch_density(const Space &sp, const SpaceTables &tb, int order,
                            const double2 *phi, const double2 *psi, double2 *partial,
-                           double2 *out, cudaStream_t st);
+                           double2 *out, cudaStream_t st, int *status = nullptr,
+                           long long wait_cycles = 0, int test_stall = 0);
 
 // Reference-layout tables built on the device.
 cudaError_t launch_focks(const Space &sp, const SpaceTables &tb, int32_t *IF, cudaStream_t st);

@@ -134,7 +134,8 @@ def test_densities_golden(golden_ops):
         sp.close()
 
 
-@pytest.mark.parametrize("N,M", [(10, 10), (7, 11), (3, 16), (1, 5), (0, 3)])
+@pytest.mark.parametrize("N,M", [(10, 10), (7, 11), (3, 16), (1, 5), (0, 3), (5, 12), (2, 12), (2, 9), (20, 3),
+                                 (30, 2), (6, 13)])
 def test_densities_oracle(orc, N, M):
     C = mc.random_problem(N, M, 21)[0]
     sp = _space(N, M)
@@ -148,16 +149,39 @@ def test_densities_oracle(orc, N, M):
     assert abs(tr - N * (N - 1)) <= 1e-12 * max(1, N * N)
 
 
-@pytest.mark.parametrize("N,M", [(5, 5), (6, 7), (2, 4)])
+@pytest.mark.parametrize("N,M", [(5, 5), (6, 7), (2, 4), (8, 10), (9, 9), (2, 10), (4, 11), (3, 12)])
 def test_transition_densities(orc, N, M):
+    # M <= 10: FP64 tensor-core Gram; larger M: the CUDA-core Gram
     phi = mc.random_problem(N, M, 31)[0]
     psi = mc.random_problem(N, M, 32)[0]
     sp = _space(N, M)
+    nc = orc.nc(N, M)
     t1 = sp.trans_rho1(phi, psi).cpu().numpy()
-    o1 = orc.density(N, M, 1, phi, psi).reshape(M, M).T      # oracle flat k + l*M
+    o1 = orc.density_rows(N, M, 1, phi, psi, 0, nc).reshape(M, M).T      # oracle flat k + l*M
     assert rel(t1, o1) <= TOL
     t2 = sp.trans_rho2(phi, psi).cpu().numpy()
-    assert rel(t2, orc.density(N, M, 2, phi, psi)) <= TOL
+    assert rel(t2, orc.density_rows(N, M, 2, phi, psi, 0, nc)) <= TOL
+
+
+def test_gram_wait_timeout_is_reported(orc):
+    # the tensor-core Gram kernel's waits are bounded: with its gather warps held
+    # back by the test switch the product warps give up after the (shortened)
+    # limit, the next synchronisation reports MCPI_ERR_TIMEOUT, and the space
+    # keeps working afterwards
+    N, M = 8, 10
+    C = mc.random_problem(N, M, 79)[0]
+    sp = _space(N, M)
+    sp.set_option(mc.OPT_WAIT_LIMIT_KCYCLES, 1000)
+    sp.set_option(mc.OPT_TEST_STALL_GATHER, 1)
+    sp.rho2(C)
+    with pytest.raises(mc.MCPIError) as err:
+        sp.sync()
+    assert err.value.status == 7      # MCPI_ERR_TIMEOUT
+    sp.set_option(mc.OPT_TEST_STALL_GATHER, 0)
+    r2 = sp.rho2(C).cpu().numpy()
+    sp.sync()
+    assert rel(r2, orc.density_rows(N, M, 2, C, C, 0, orc.nc(N, M))) <= TOL
+    sp.close()
 
 
 def test_energy_identity_device():
