@@ -22,7 +22,12 @@ this size) on a bounded row sample with all host threads.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mcpi|reference]
 
 With --gpus N > 1 (under torchrun) each rank runs an independent replica of
-the workload on its own GPU (the solve does not shard: weak scaling).
+the H.psi workload on its own GPU (weak scaling); the `sharded` section runs
+one row-sharded Lanczos solve across all ranks (NCCL all-gather of each new
+Krylov vector and all-reduces of the dots; at N=1 a one-rank group), timed end
+to end from a pinned host start vector to the energy and Ritz shard on the
+host. The `adjoint` section times H.psi, its adjoint and the transition
+densities at N=8, M=8.
 `--impl reference` times the CPU oracle port alone (rank 0), on the same
 config, metric and unit.
 """
@@ -59,6 +64,8 @@ def parse():
     p.add_argument("--no-batch", action="store_true")
     p.add_argument("--no-large", action="store_true")
     p.add_argument("--no-general", action="store_true")
+    p.add_argument("--no-sharded", action="store_true")
+    p.add_argument("--no-adjoint", action="store_true")
     p.add_argument("--profile", choices=["batch", "lanczos", "density"], default=None,
                    help="run only this section (for profiler launch lists), print its timings")
     return p.parse_args()
@@ -79,7 +86,9 @@ def config(extra=None):
 # ---------------------------------------------------------------------------
 
 class Clocks:
-    """nvidia-smi sampling during the timed region."""
+    """nvidia-smi sampling during the timed region. start() returns once the
+    sampler has written its first row (nvidia-smi takes about a second to come
+    up), and only the rows written after that count."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -87,26 +96,45 @@ class Clocks:
     def __init__(self, device):
         self.device = device
         self.proc = None
+        self.n0 = 0
+
+    def _target(self):
+        """nvidia-smi -i selector of the torch device: its PCI bus id where torch has it."""
+        try:
+            import torch
+            p = torch.cuda.get_device_properties(self.device)
+            return f"{p.pci_domain_id:08X}:{p.pci_bus_id:02X}:{p.pci_device_id:02X}.0"
+        except Exception:
+            return str(self.device)
+
+    def _rows(self):
+        self.f.flush()
+        return [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
 
     def start(self):
         self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                 "-i", str(self.device), "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+                 "-i", self._target(), "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
+            return
+        t0 = time.time()
+        while time.time() - t0 < 10.0 and self.proc.poll() is None and not self._rows():
+            time.sleep(0.05)
+        self.n0 = len(self._rows())
 
     def stop(self):
         if self.proc is None:
             return None
+        time.sleep(0.15)   # one more sample interval
         self.proc.terminate()
         try:
             self.proc.wait(5)
         except subprocess.TimeoutExpired:
             self.proc.kill()
-        self.f.flush()
-        rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
+        rows = self._rows()[self.n0:]
         os.unlink(self.f.name)
         sm, mx, reasons = [], 0.0, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
@@ -209,6 +237,84 @@ def run_batch(mc, torch, device, iters=120):
             "max_rel_dE0_vs_sequential": dE, "steps_done_min": int(it.min()),
             "nc_min": min(ncs), "nc_max": max(ncs), "arena_gb": arena / 1e9,
             "tile_rows": tile, "tile_probe_ms": {str(t): float(x) for t, x in zip((512, 1024, 2048), tune_ms)}}
+
+
+def run_sharded(mc, torch, dev, local, world, rank, barrier, max_over_ranks, iters=LANCZOS_ITERS):
+    """The row-sharded Lanczos ground state (mcpi_b200/distributed.py) of the
+    N=16, M=10 workload over all ranks (NCCL; at one GPU a one-rank group):
+    each rank owns nc / world rows of every Krylov vector, all-gathers the new
+    vector each step and runs its rows' H.psi and its shard of the
+    reorthogonalisation in the library's kernels. Timed end to end: the start
+    vector's shard comes from pinned host memory and the ground-state energy
+    and Ritz-vector shard go back to the host."""
+    import socket
+
+    import torch.distributed as dist
+
+    from mcpi_b200.distributed import ShardedLanczos
+    own = not dist.is_initialized()
+    if own:
+        s = socket.socket()
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+        s.close()
+        dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1)
+    try:
+        N, M = N_PART, M_ORB
+        sp = mc.FockSpace(N, M, device=local)
+        sp.set_integrals(*mc.lieb_integrals(M, G, L_RING))
+        sl = ShardedLanczos(sp.nc, lambda v: sp.apply_h_rows(v, sl.r0, sl.r1), dev)
+        rng = np.random.default_rng(4321)
+        C0 = rng.standard_normal(sp.nc) + 1j * rng.standard_normal(sp.nc)
+        C0 /= np.linalg.norm(C0)
+        host = torch.from_numpy(C0[sl.r0:sl.r1].copy()).pin_memory()
+        sl.ground(host.to(dev), iters)                    # warm-up
+        torch.cuda.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        E0, psi, it = sl.ground(host.to(dev, non_blocking=True), iters)
+        psi_h = psi.cpu()
+        dt = max_over_ranks(time.perf_counter() - t0)
+        n = sl.r1 - sl.r0
+        sp.close()
+        return {"ranks": world, "rows_per_rank": n, "iterations": it, "E0": E0, "seconds": dt,
+                "solves_per_s": 1.0 / dt,
+                "e2e": {"value": 1.0 / dt, "unit": "solves/s", "h2d_bytes_per_step": 16 * n,
+                        "d2h_bytes_per_step": 16 * n + 8, "api": "ShardedLanczos.ground (mcpi_shard_*, NCCL)"},
+                "ritz_shard_norm2": float((psi_h.abs() ** 2).sum())}
+    finally:
+        if own:
+            dist.destroy_process_group()
+
+
+def run_adjoint(mc, torch, device, reps=200):
+    """The adjoint configuration (N=8, M=8, nc = 6,435; random Hermitian Ho and
+    8-fold symmetrised Hint): H.psi, its adjoint and the transition densities
+    that give the gradients with respect to Ho and Hint, timed with CUDA
+    events (mean over reps calls)."""
+    N, M = 8, 8
+    C, Ho, Hint = mc.random_problem(N, M, 8)
+    phi = mc.random_problem(N, M, 9)[0]
+    sp = mc.FockSpace(N, M, device=device)
+    sp.set_integrals(Ho, Hint)
+    x = torch.from_numpy(C).to(sp.torch_device)
+    y = torch.from_numpy(phi).to(sp.torch_device)
+    out = sp.empty()
+    res = {"N": N, "M": M, "nc": sp.nc}
+    for name, f in (("apply_h", lambda: sp.apply_h(x, out)), ("apply_h_adjoint", lambda: sp.apply_h_adjoint(y)),
+                    ("trans_rho1", lambda: sp.trans_rho1(y, x)), ("trans_rho2", lambda: sp.trans_rho2(y, x))):
+        for _ in range(5):
+            f()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            f()
+        b.record()
+        torch.cuda.synchronize()
+        res[name + "_us"] = a.elapsed_time(b) / reps * 1e3
+    sp.close()
+    return res
 
 
 def run_large(mc, torch, device):
@@ -478,8 +584,13 @@ def run_mcpi(args):
     ms = max_over_ranks(e0.elapsed_time(e1))
     value = world * args.steps / (ms / 1e3)
 
-    # ---- roofline of the dominant kernel (CUDA events on the launching stream) ----
-    k1, k2 = sp.apply_h_profile(X[0], out, reps=20)
+    # ---- roofline of the dominant kernel (CUDA events on the launching stream,
+    # the same rotating states as the timed region) ----
+    k1 = k2 = 0.0
+    for k in range(2 * ROTATE):
+        a, b = sp.apply_h_profile(X[k % ROTATE], out, reps=1)
+        k1 += a / (2 * ROTATE)
+        k2 += b / (2 * ROTATE)
     names = ["pair_annihilate", "pair_create"]
     times = {"pair_annihilate": k1, "pair_create": k2}
     dom = max(names, key=lambda n: times[n])
@@ -547,6 +658,15 @@ def run_mcpi(args):
         lanczos = {"iterations": it, "E0": E0, "E0_per_N": E0 / N, "seconds": dt,
                    "solves_per_s": world / dt, "occupations": [round(float(o), 6) for o in occ]}
 
+    sharded = None
+    if not args.no_sharded:
+        sharded = run_sharded(mc, torch, dev, local, world, rank, barrier, max_over_ranks)
+        if lanczos is not None:
+            sharded["single_gpu_seconds"] = lanczos["seconds"]
+    adjoint = None
+    if not args.no_adjoint:
+        adjoint = run_adjoint(mc, torch, local)
+
     batched = None
     if not args.no_batch:
         batched = run_batch(mc, torch, local)
@@ -566,8 +686,8 @@ def run_mcpi(args):
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
                 "config": config(), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-                "gpu_launches": 2 * args.steps, "clocks": clk, "lanczos": lanczos, "batched": batched,
-                "large": large, "general": general}
+                "gpu_launches": 2 * args.steps, "clocks": clk, "lanczos": lanczos, "sharded": sharded,
+                "adjoint": adjoint, "batched": batched, "large": large, "general": general}
         print(json.dumps(line), flush=True)
     sp.close()
     if world > 1:

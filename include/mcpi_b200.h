@@ -148,7 +148,10 @@ MCPI_API int mcpi_apply_h(mcpi_space sp, const void *d_C, void *d_out);
 MCPI_API int mcpi_apply_h_host(mcpi_space sp, int count, const void *const *h_C, void *const *h_out);
 /* Rows [row0, row1) of H C into d_out[0 .. row1-row0), d_C being the whole
  * vector: the local part of a row-sharded H.psi (each rank owns a row block
- * and gathers the full vector first). Needs N >= 2. No reference counterpart. */
+ * and gathers the full vector first). Needs N >= 2. No reference counterpart.
+ * With momentum-block integrals the pair-annihilation kernel runs only over
+ * the (N-2)-configurations these rows read (found on the first call for a row
+ * block, which synchronises the space's stream once). */
 MCPI_API int mcpi_apply_h_rows(mcpi_space sp, const void *d_C, int64_t row0, int64_t row1, void *d_out);
 /* mcpi_apply_h, timed: runs it reps times with CUDA events around each of its
  * two kernels on the space's stream (synchronising after every repetition) and
@@ -189,6 +192,42 @@ MCPI_API int mcpi_trans_rho1(mcpi_space sp, const void *d_phi, const void *d_psi
 MCPI_API int mcpi_trans_rho2(mcpi_space sp, const void *d_phi, const void *d_psi, void *d_t2);
 /* <a, b> = sum conj(a) b (groundStateLieb.c:73-85, carrDot), host result. */
 MCPI_API int mcpi_dot(mcpi_space sp, const void *d_a, const void *d_b, double *h_result2);
+
+/* Row-shard Lanczos primitives. No counterpart in the reference, whose
+ * lanczos (groundStateLieb.c:217-344) runs in one process: here a process per
+ * GPU owns rows [row0, row1) of every Krylov vector (n = row1 - row0, its
+ * shard) and runs the reference's recurrence with these calls, summing each
+ * per-rank result (dot, coefficients, norm^2) over the ranks with an
+ * all-reduce between the calls (mcpi_b200/distributed.py is the driver; the
+ * H.psi of a shard is mcpi_apply_h_rows on the all-gathered vector). All
+ * scalars stay in device memory, so a solve needs no host round trip; every
+ * kernel returns at entry once *d_done != 0, so all ranks keep issuing the
+ * same collectives after a breakdown. Sums inside a rank run in a fixed
+ * order. Device pointers (complex = 2 doubles), work on `stream`.
+ *   scratch: mcpi_shard_scratch_elems(n, lm) complex entries. */
+MCPI_API size_t mcpi_shard_scratch_elems(int64_t n, int lm);
+/* vnext = r / *beta_i */
+MCPI_API int mcpi_shard_scale(int64_t n, const void *d_r, void *d_vnext, const double *d_beta_i,
+                              const int *d_done, void *stream);
+/* r -= *beta_i vprev (skipped when d_vprev is NULL); *d_dot = <vcur, r> over the shard */
+MCPI_API int mcpi_shard_axpy_dot(int64_t n, const void *d_vprev, const void *d_vcur, void *d_r,
+                                 const double *d_beta_i, void *d_scratch, void *d_dot, const int *d_done,
+                                 void *stream);
+/* coef[j] = <V_j, r - alpha vcur> over the shard, j < nvec (V: nvec shards of n) */
+MCPI_API int mcpi_shard_multidot(int64_t n, const void *d_V, int nvec, const void *d_r, const void *d_vcur,
+                                 const void *d_alpha, void *d_scratch, void *d_coef, const int *d_done,
+                                 void *stream);
+/* r = r - alpha vcur - sum_j coef[j] V_j (nvec may be 0); *d_norm2 = |r|^2 over the shard */
+MCPI_API int mcpi_shard_update(int64_t n, const void *d_V, int nvec, void *d_r, const void *d_vcur,
+                               const void *d_alpha, const void *d_coef, void *d_scratch, double *d_norm2,
+                               const int *d_done, void *stream);
+/* beta[i] = sqrt(*d_norm2) (summed over the ranks) and the breakdown test of
+ * groundStateLieb.c:287-292: sets *d_done = 1 and *d_iters = i */
+MCPI_API int mcpi_shard_beta(int i, double tol, const double *d_norm2, double *d_beta, double *d_maxbeta,
+                             int *d_done, int *d_iters, void *stream);
+/* out = sum_k V_k z[k], k < nvec (z real, device) -- a shard of the Ritz vector */
+MCPI_API int mcpi_shard_combine(int64_t n, const void *d_V, int nvec, const double *d_z, void *d_out,
+                                void *stream);
 
 /* ---- Lanczos (groundStateLieb.c:217-471) ------------------------------------ */
 /* Lanczos with full classical Gram-Schmidt reorthogonalisation

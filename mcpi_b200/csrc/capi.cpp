@@ -530,6 +530,7 @@ int mcpi_space_destroy(mcpi_space sp)
     cudaFree(sp->d_lzr);
     free_host_pipe(sp);
     free_fused(sp);
+    cudaFree(sp->d_mr);
     if (sp->own) cudaStreamDestroy(sp->own);
     delete sp;
     return MCPI_OK;
@@ -915,8 +916,28 @@ int mcpi_apply_h_rows(mcpi_space sp, const void *d_C, int64_t row0, int64_t row1
     DeviceGuard g(sp->device);
     int rc = ensure_E(sp);
     if (rc) return rc;
+    // kernel 1 only over the E columns these rows read (momentum-block form):
+    // a rank of a sharded solve does not recompute the whole intermediate.
+    // The range is found once per row block (one pass over its rows).
+    uint32_t m0 = 0, m1 = 0xffffffffu;
+    if (sp->fwd.hblk && sp->M >= 2) {
+        if (sp->mr_r0 != row0 || sp->mr_r1 != row1) {
+            if (!sp->d_mr) CK(cudaMalloc(&sp->d_mr, 2 * sizeof(uint32_t)));
+            uint32_t h[2];
+            CK(mcpi::launch_rows_mrange(sp->sp, sp->tables(), (uint32_t)row0, (uint32_t)row1, sp->d_mr, sp->stream));
+            CK(cudaMemcpyAsync(h, sp->d_mr, sizeof h, cudaMemcpyDeviceToHost, sp->stream));
+            CK(cudaStreamSynchronize(sp->stream));
+            if (h[0] > h[1] || h[1] >= sp->nc2) return fail(MCPI_ERR_CUDA, "row block range: bad columns");
+            sp->mr_r0 = row0;
+            sp->mr_r1 = row1;
+            sp->mr_lo = h[0];
+            sp->mr_hi = h[1];
+        }
+        m0 = sp->mr_lo;
+        m1 = sp->mr_hi + 1;
+    }
     CK(mcpi::launch_apply_h(sp->sp, sp->tables(), sp->fwd.view(), sp->fwd.blocks(), (const double2 *)d_C,
-                            sp->d_E, (double2 *)d_out, sp->stream, 3, (uint32_t)row0, (uint32_t)row1));
+                            sp->d_E, (double2 *)d_out, sp->stream, 3, (uint32_t)row0, (uint32_t)row1, m0, m1));
     return MCPI_OK;
 }
 
@@ -941,6 +962,76 @@ int mcpi_rho1(mcpi_space sp, const void *d_C, void *d_rho1) { return density(sp,
 int mcpi_rho2(mcpi_space sp, const void *d_C, void *d_rho2) { return density(sp, 2, d_C, d_C, d_rho2); }
 int mcpi_trans_rho1(mcpi_space sp, const void *phi, const void *psi, void *t1) { return density(sp, 1, phi, psi, t1); }
 int mcpi_trans_rho2(mcpi_space sp, const void *phi, const void *psi, void *t2) { return density(sp, 2, phi, psi, t2); }
+
+// ---- row-shard Lanczos primitives ------------------------------------------------------
+
+#define SHARD_CK(call)                                                                      \
+    do {                                                                                    \
+        cudaError_t _e = (call);                                                            \
+        if (_e != cudaSuccess) return fail(MCPI_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(_e)); \
+    } while (0)
+
+size_t mcpi_shard_scratch_elems(int64_t n, int lm) { return n < 0 || lm < 1 ? 0 : mcpi::shard_scratch_elems(n, lm); }
+
+int mcpi_shard_scale(int64_t n, const void *d_r, void *d_vnext, const double *d_beta_i, const int *d_done,
+                     void *stream)
+{
+    CHECK_ARG(n >= 0 && d_r && d_vnext && d_beta_i && d_done, "mcpi_shard_scale: bad arguments");
+    if (n == 0) return MCPI_OK;
+    SHARD_CK(mcpi::launch_shard_scale(n, (const double2 *)d_r, (double2 *)d_vnext, d_beta_i, d_done,
+                                      (cudaStream_t)stream));
+    return MCPI_OK;
+}
+
+int mcpi_shard_axpy_dot(int64_t n, const void *d_vprev, const void *d_vcur, void *d_r, const double *d_beta_i,
+                        void *d_scratch, void *d_dot, const int *d_done, void *stream)
+{
+    CHECK_ARG(n >= 0 && d_vcur && d_r && d_scratch && d_dot && d_done && (!d_vprev || d_beta_i),
+              "mcpi_shard_axpy_dot: bad arguments");
+    SHARD_CK(mcpi::launch_shard_axpy_dot(n, (const double2 *)d_vprev, (const double2 *)d_vcur, (double2 *)d_r,
+                                         d_beta_i, (double2 *)d_scratch, (double2 *)d_dot, d_done,
+                                         (cudaStream_t)stream));
+    return MCPI_OK;
+}
+
+int mcpi_shard_multidot(int64_t n, const void *d_V, int nvec, const void *d_r, const void *d_vcur,
+                        const void *d_alpha, void *d_scratch, void *d_coef, const int *d_done, void *stream)
+{
+    CHECK_ARG(n >= 0 && nvec >= 1 && d_V && d_r && d_vcur && d_alpha && d_scratch && d_coef && d_done,
+              "mcpi_shard_multidot: bad arguments");
+    SHARD_CK(mcpi::launch_shard_multidot(n, (const double2 *)d_V, nvec, (const double2 *)d_r,
+                                         (const double2 *)d_vcur, (const double2 *)d_alpha, (double2 *)d_scratch,
+                                         (double2 *)d_coef, d_done, (cudaStream_t)stream));
+    return MCPI_OK;
+}
+
+int mcpi_shard_update(int64_t n, const void *d_V, int nvec, void *d_r, const void *d_vcur, const void *d_alpha,
+                      const void *d_coef, void *d_scratch, double *d_norm2, const int *d_done, void *stream)
+{
+    CHECK_ARG(n >= 0 && nvec >= 0 && (nvec == 0 || (d_V && d_coef)) && d_r && d_vcur && d_alpha && d_scratch &&
+                  d_norm2 && d_done,
+              "mcpi_shard_update: bad arguments");
+    SHARD_CK(mcpi::launch_shard_update(n, (const double2 *)d_V, nvec, (double2 *)d_r, (const double2 *)d_vcur,
+                                       (const double2 *)d_alpha, (const double2 *)d_coef, (double2 *)d_scratch,
+                                       d_norm2, d_done, (cudaStream_t)stream));
+    return MCPI_OK;
+}
+
+int mcpi_shard_beta(int i, double tol, const double *d_norm2, double *d_beta, double *d_maxbeta, int *d_done,
+                    int *d_iters, void *stream)
+{
+    CHECK_ARG(i >= 0 && d_norm2 && d_beta && d_maxbeta && d_done && d_iters, "mcpi_shard_beta: bad arguments");
+    SHARD_CK(mcpi::launch_shard_beta(i, tol, d_norm2, d_beta, d_maxbeta, d_done, d_iters, (cudaStream_t)stream));
+    return MCPI_OK;
+}
+
+int mcpi_shard_combine(int64_t n, const void *d_V, int nvec, const double *d_z, void *d_out, void *stream)
+{
+    CHECK_ARG(n >= 0 && nvec >= 1 && d_V && d_z && d_out, "mcpi_shard_combine: bad arguments");
+    if (n == 0) return MCPI_OK;
+    SHARD_CK(mcpi::launch_combine((const double2 *)d_V, nvec, n, d_z, (double2 *)d_out, (cudaStream_t)stream));
+    return MCPI_OK;
+}
 
 int mcpi_dot(mcpi_space sp, const void *d_a, const void *d_b, double *h_result2)
 {

@@ -714,11 +714,13 @@ __device__ __forceinline__ void annihilate_momentum_row(const Space &sp, const S
     }
 }
 
+// Configurations m0 + block * kT2 + t below m1 (the whole space: 0, nc2).
 template <int M, bool PARAM = false>
 __device__ __forceinline__ void annihilate_momentum_body(const Space &sp, const SpaceTables &tb,
                                                          const double2 *__restrict__ hblk, int nh,
                                                          const double2 *__restrict__ psi,
-                                                         double2 *__restrict__ E, uint32_t block)
+                                                         double2 *__restrict__ E, uint32_t block,
+                                                         uint32_t m0 = 0, uint32_t m1 = 0xffffffffu)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double2 *hs = reinterpret_cast<double2 *>(smem_raw);          // nh (staged form only)
@@ -730,8 +732,8 @@ __device__ __forceinline__ void annihilate_momentum_body(const Space &sp, const 
     const double2 *hv = PARAM ? hblk : hs;
     __syncthreads();
 
-    const uint32_t m = block * kT2 + threadIdx.x;
-    if (m >= sp.nc2) return;
+    const uint32_t m = m0 + block * kT2 + threadIdx.x;
+    if (m >= sp.nc2 || m >= m1) return;
     annihilate_momentum_row<M, kEStoreStream>(sp, tb, W, sq, hv, psi, E, m, 0);
 }
 
@@ -740,9 +742,10 @@ __global__ void __launch_bounds__(kT2, 3) k_pair_annihilate_momentum(Space sp, S
                                                                   const double2 *__restrict__ hblk,
                                                                   int nh,
                                                                   const double2 *__restrict__ psi,
-                                                                  double2 *__restrict__ E)
+                                                                  double2 *__restrict__ E, uint32_t m0,
+                                                                  uint32_t m1)
 {
-    annihilate_momentum_body<M>(sp, tb, hblk, nh, psi, E, blockIdx.x);
+    annihilate_momentum_body<M>(sp, tb, hblk, nh, psi, E, blockIdx.x, m0, m1);
 }
 
 // Number of momentum-block values for M orbitals (sum over K of block size squared).
@@ -766,9 +769,10 @@ template <int M>
 __global__ void __launch_bounds__(kT2, 3) k_pair_annihilate_momentum_p(Space sp, SpaceTables tb,
                                                                     const __grid_constant__ MomBlocks<M> hp,
                                                                     const double2 *__restrict__ psi,
-                                                                    double2 *__restrict__ E)
+                                                                    double2 *__restrict__ E, uint32_t m0,
+                                                                    uint32_t m1)
 {
-    annihilate_momentum_body<M, true>(sp, tb, hp.v, mom_values<M>(), psi, E, blockIdx.x);
+    annihilate_momentum_body<M, true>(sp, tb, hp.v, mom_values<M>(), psi, E, blockIdx.x, m0, m1);
 }
 
 // ---------------------------------------------------------------------------
@@ -1294,7 +1298,7 @@ __global__ void k_one_particle(int M, const double2 *__restrict__ hfull,
 template <int M>
 cudaError_t apply_h_m(const Space &sp, const SpaceTables &tb, const PairOp &op, const BlockOp &bo,
                       const double2 *psi, double2 *E, double2 *out, int stages, cudaStream_t st,
-                      uint32_t row0, uint32_t row1)
+                      uint32_t row0, uint32_t row1, uint32_t m0, uint32_t m1)
 {
     constexpr int P = M * (M + 1) / 2;
     const size_t tab = sizeof(double) * sp.wstride + sizeof(uint32_t) * (M - 1) * sp.wstride;
@@ -1304,14 +1308,16 @@ cudaError_t apply_h_m(const Space &sp, const SpaceTables &tb, const PairOp &op, 
             return fused_apply_m<M>(sp, tb, op, psi, E, out, st);
     }
     if (sp.N >= 2 && (stages & 1) && op.hblk) {
-        const unsigned g1 = (sp.nc2 + kT2 - 1) / kT2;
-        if (op.hblk_host && op.nhblk == mom_values<M>()) {
+        // only the configurations [m0, m1) (a row block's range; the whole space by default)
+        if (m1 > sp.nc2) m1 = sp.nc2;
+        const unsigned g1 = m1 > m0 ? (m1 - m0 + kT2 - 1) / kT2 : 0;
+        if (g1 && op.hblk_host && op.nhblk == mom_values<M>()) {
             MomBlocks<M> hp;
             for (int x = 0; x < mom_values<M>(); ++x) hp.v[x] = op.hblk_host[x];
-            k_pair_annihilate_momentum_p<M><<<g1, kT2, tab, st>>>(sp, tb, hp, psi, E);
-        } else {
+            k_pair_annihilate_momentum_p<M><<<g1, kT2, tab, st>>>(sp, tb, hp, psi, E, m0, m1);
+        } else if (g1) {
             const size_t smm = sizeof(double2) * op.nhblk + tab;
-            k_pair_annihilate_momentum<M><<<g1, kT2, smm, st>>>(sp, tb, op.hblk, op.nhblk, psi, E);
+            k_pair_annihilate_momentum<M><<<g1, kT2, smm, st>>>(sp, tb, op.hblk, op.nhblk, psi, E, m0, m1);
         }
     } else if (sp.N >= 2 && (stages & 1) && bo.prog) {
         const size_t smb = ((bo.bytes + 15) & ~15) + (2 * sizeof(double) + 2 * sizeof(uint32_t)) * M * kT1b + tab;
@@ -1443,6 +1449,80 @@ size_t batch_smem(int M, int N, int nh, int stage)
 
 int batch_rows_per_block(int stage) { return stage == 1 ? kT2 : kTC; }
 
+namespace {
+
+// The (N-2)-configurations rows [r0, r1) read in kernel 2: every row reads
+// index(v - e_k - e_s) for its occupied pairs, the largest from its two lowest
+// particles and the smallest from its two highest (the top occupation is the
+// most significant digit of the index order). out[0] = min, out[1] = max
+// (initialised by the caller to UINT32_MAX and 0).
+template <int M>
+__global__ void __launch_bounds__(kFusedTile) k_rows_mrange(Space sp, SpaceTables tb, uint32_t r0, uint32_t r1,
+                                                            uint32_t *out)
+{
+    extern __shared__ uint32_t Wr[];   // (M-1) x wstride
+    const int ws = sp.wstride;
+    for (int x = threadIdx.x; x < (M - 1) * ws; x += blockDim.x) Wr[x] = tb.W[x];
+    __syncthreads();
+    const uint32_t i = r0 + blockIdx.x * kFusedTile + threadIdx.x;
+    uint32_t lo = 0xffffffffu, hi = 0u;
+    if (i < r1) {
+        int v[M], P[M];
+        occupations<M>(tb.occ, tb.occ_bits, i, sp.N, sp.nc, Wr, ws, v, P);
+        int k0 = 0;
+        while (k0 < M - 1 && v[k0] == 0) ++k0;
+        int k1 = k0;
+        if (v[k0] < 2) {
+            k1 = k0 + 1;
+            while (k1 < M - 1 && v[k1] == 0) ++k1;
+        }
+        int s1 = M - 1;
+        while (s1 > 0 && v[s1] == 0) --s1;
+        int s0 = s1;
+        if (v[s1] < 2) {
+            s0 = s1 - 1;
+            while (s0 > 0 && v[s0] == 0) --s0;
+        }
+        uint32_t A0[M], Am1[M], Am2[M];
+        prefix_table<M>(P, 0, Wr, ws, A0);
+        prefix_table<M>(P, -1, Wr, ws, Am1);
+        prefix_table<M>(P, -2, Wr, ws, Am2);
+        hi = idx_remove2(sp.nc2, A0, Am1, Am2, k0, k1, M);
+        lo = idx_remove2(sp.nc2, A0, Am1, Am2, s0, s1, M);
+    }
+    for (int o = 16; o; o >>= 1) {
+        const uint32_t a = __shfl_down_sync(0xffffffffu, lo, o), b = __shfl_down_sync(0xffffffffu, hi, o);
+        lo = a < lo ? a : lo;
+        hi = b > hi ? b : hi;
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(out, lo);
+        atomicMax(out + 1, hi);
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_rows_mrange(const Space &sp, const SpaceTables &tb, uint32_t r0, uint32_t r1, uint32_t *out,
+                               cudaStream_t st)
+{
+    if (sp.N < 2 || sp.M < 2 || r1 <= r0 || r1 > sp.nc) return cudaErrorInvalidValue;
+    const uint32_t init[2] = {0xffffffffu, 0u};
+    cudaError_t e = cudaMemcpyAsync(out, init, sizeof init, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) return e;
+    const unsigned g = (r1 - r0 + kFusedTile - 1) / kFusedTile;
+    const size_t sm = sizeof(uint32_t) * (sp.M - 1) * sp.wstride;
+    switch (sp.M) {
+#define MCPI_CASE(m) \
+    case m: k_rows_mrange<m><<<g, kFusedTile, sm, st>>>(sp, tb, r0, r1, out); return cudaGetLastError();
+        MCPI_CASE(2) MCPI_CASE(3) MCPI_CASE(4) MCPI_CASE(5) MCPI_CASE(6) MCPI_CASE(7) MCPI_CASE(8)
+        MCPI_CASE(9) MCPI_CASE(10) MCPI_CASE(11) MCPI_CASE(12) MCPI_CASE(13) MCPI_CASE(14)
+        MCPI_CASE(15) MCPI_CASE(16)
+#undef MCPI_CASE
+    default: return cudaErrorInvalidValue;
+    }
+}
+
 cudaError_t launch_fused_need(const Space &sp, const SpaceTables &tb, int *need, cudaStream_t st)
 {
     if (sp.N < 2 || sp.M < 2) return cudaErrorInvalidValue;
@@ -1474,7 +1554,8 @@ cudaError_t fused_config(const Space &sp, int *grid, size_t *smem)
 
 cudaError_t launch_apply_h(const Space &sp, const SpaceTables &tb, const PairOp &op,
                            const BlockOp &bo, const double2 *psi, double2 *E, double2 *out,
-                           cudaStream_t st, int stages, uint32_t row0, uint32_t row1)
+                           cudaStream_t st, int stages, uint32_t row0, uint32_t row1, uint32_t m0,
+                           uint32_t m1)
 {
     if (row1 == 0xffffffffu) row1 = sp.nc;
     if (row0 > row1 || row1 > sp.nc) return cudaErrorInvalidValue;
@@ -1485,7 +1566,7 @@ cudaError_t launch_apply_h(const Space &sp, const SpaceTables &tb, const PairOp 
     }
     switch (sp.M) {
 #define MCPI_CASE(m) \
-    case m: return apply_h_m<m>(sp, tb, op, bo, psi, E, out, stages, st, row0, row1);
+    case m: return apply_h_m<m>(sp, tb, op, bo, psi, E, out, stages, st, row0, row1, m0, m1);
         MCPI_CASE(1) MCPI_CASE(2) MCPI_CASE(3) MCPI_CASE(4) MCPI_CASE(5) MCPI_CASE(6)
         MCPI_CASE(7) MCPI_CASE(8) MCPI_CASE(9) MCPI_CASE(10) MCPI_CASE(11) MCPI_CASE(12)
         MCPI_CASE(13) MCPI_CASE(14) MCPI_CASE(15) MCPI_CASE(16)

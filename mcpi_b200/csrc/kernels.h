@@ -98,10 +98,17 @@ cudaError_t launch_pack_occ(const Space &sp, const SpaceTables &tb, uint64_t *oc
 // row0/row1: with the default shared-table creation kernel, only rows
 // [row0, row1) of out are computed, into out[0 .. row1-row0) (psi stays the
 // full vector); 0xffffffff = nc.
+// m0/m1: with the momentum-block form, kernel 1 runs only over the
+// (N-2)-configurations [m0, m1) -- the E columns a row range reads
+// (launch_rows_mrange); other forms always run over the whole space.
 cudaError_t launch_apply_h(const Space &sp, const SpaceTables &tb, const PairOp &op,
                            const BlockOp &bo, const double2 *psi, double2 *E, double2 *out,
                            cudaStream_t st, int stages = 3, uint32_t row0 = 0,
-                           uint32_t row1 = 0xffffffffu);
+                           uint32_t row1 = 0xffffffffu, uint32_t m0 = 0, uint32_t m1 = 0xffffffffu);
+// out[0], out[1] (device) = the lowest and highest (N-2)-configuration that
+// rows [r0, r1) read in kernel 2.
+cudaError_t launch_rows_mrange(const Space &sp, const SpaceTables &tb, uint32_t r0, uint32_t r1, uint32_t *out,
+                               cudaStream_t st);
 
 // Fused H.psi set-up: need[c] = the highest producer tile consumer tile c
 // reads (device, ceil(nc / kFusedTile) entries); the persistent grid and
@@ -199,5 +206,23 @@ cudaError_t launch_lanczos_axpy(const double2 *vprev, double2 *r, int64_t nc, in
                                cudaStream_t st);
 cudaError_t launch_dot(const double2 *a, const double2 *b, int64_t nc, double2 *partial,
                        double2 *result, cudaStream_t st);
+
+// Row-shard primitives of a sharded Lanczos (n rows of this rank; scalars on the
+// device; every kernel returns at entry once *done != 0). The caller sums the
+// per-rank results (dot, coef, norm2) over the ranks between the calls.
+size_t shard_scratch_elems(int64_t n, int lm);
+cudaError_t launch_shard_scale(int64_t n, const double2 *r, double2 *vnext, const double *beta_i, const int *done,
+                               cudaStream_t st);
+cudaError_t launch_shard_axpy_dot(int64_t n, const double2 *vprev, const double2 *vcur, double2 *r,
+                                  const double *beta_i, double2 *scratch, double2 *dot, const int *done,
+                                  cudaStream_t st);
+cudaError_t launch_shard_multidot(int64_t n, const double2 *V, int nvec, const double2 *r, const double2 *vcur,
+                                  const double2 *alpha, double2 *scratch, double2 *coef, const int *done,
+                                  cudaStream_t st);
+cudaError_t launch_shard_update(int64_t n, const double2 *V, int nvec, double2 *r, const double2 *vcur,
+                                const double2 *alpha, const double2 *coef, double2 *scratch, double *norm2,
+                                const int *done, cudaStream_t st);
+cudaError_t launch_shard_beta(int i, double tol, const double *norm2, double *beta, double *maxbeta, int *done,
+                              int *iters, cudaStream_t st);
 
 }  // namespace mcpi

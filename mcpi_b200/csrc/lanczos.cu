@@ -251,6 +251,30 @@ __global__ void k_beta(const double2 *__restrict__ partial, int n, int i, double
     }
 }
 
+// The same test from a norm^2 already summed over the ranks of a sharded solve.
+__global__ void k_beta_total(const double *norm2, int i, double tol, double *beta, double *maxbeta, int *done,
+                             int *iters)
+{
+    if (*done || threadIdx.x != 0) return;
+    const double bi = sqrt(*norm2);
+    beta[i] = bi;
+    if (*maxbeta < bi) *maxbeta = bi;
+    if (!(bi / *maxbeta >= tol)) {
+        *done = 1;
+        *iters = i;
+    }
+}
+
+// *out = real part of sum_b partial[b] (b in order); one block.
+__global__ void k_sum_partials_re(const double2 *__restrict__ partial, int n, double *out, const int *done)
+{
+    if (stopped(done)) return;
+    double2 acc = make_double2(0.0, 0.0);
+    for (int b = threadIdx.x; b < n; b += kThreads) acc.x += partial[b].x;
+    acc = block_sum(acc);
+    if (threadIdx.x == 0) *out = acc.x;
+}
+
 __global__ void k_scale(const double2 *__restrict__ r, double2 *__restrict__ vnext, int64_t n,
                         const double *beta_i, const int *done)
 {
@@ -400,6 +424,58 @@ cudaError_t launch_axpy_real(double2 *acc, const double2 *v, int64_t nc, const d
                              cudaStream_t st)
 {
     k_axpy_real<<<grid_for(nc), kThreads, 0, st>>>(acc, v, nc, z, first, nullptr);
+    return cudaGetLastError();
+}
+
+// ---- row-shard primitives (one rank's rows of a sharded solve) --------------------
+
+size_t shard_scratch_elems(int64_t n, int lm) { return lanczos_partial_elems(n, lm); }
+
+cudaError_t launch_shard_scale(int64_t n, const double2 *r, double2 *vnext, const double *beta_i, const int *done,
+                               cudaStream_t st)
+{
+    k_scale<<<grid_for(n), kThreads, 0, st>>>(r, vnext, n, beta_i, done);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_shard_axpy_dot(int64_t n, const double2 *vprev, const double2 *vcur, double2 *r,
+                                  const double *beta_i, double2 *scratch, double2 *dot, const int *done,
+                                  cudaStream_t st)
+{
+    const unsigned g = grid_for(n);
+    if (vprev)
+        k_axpy_dot<<<g, kThreads, 0, st>>>(vprev, vcur, r, n, beta_i, scratch, done);
+    else
+        k_dot_partial<<<g, kThreads, 0, st>>>(vcur, r, n, scratch, done);
+    k_sum_partials<<<1, kThreads, 0, st>>>(scratch, g, dot, done);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_shard_multidot(int64_t n, const double2 *V, int nvec, const double2 *r, const double2 *vcur,
+                                  const double2 *alpha, double2 *scratch, double2 *coef, const int *done,
+                                  cudaStream_t st)
+{
+    const unsigned nblk = (unsigned)((n + kSlice - 1) / kSlice);
+    k_multidot<<<nblk ? nblk : 1, kThreads, 0, st>>>(V, nvec, n, r, vcur, alpha, scratch, done);
+    k_multidot_finish<<<(nvec + 7) / 8, kThreads, 0, st>>>(scratch, nblk, nvec, coef, done);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_shard_update(int64_t n, const double2 *V, int nvec, double2 *r, const double2 *vcur,
+                                const double2 *alpha, const double2 *coef, double2 *scratch, double *norm2,
+                                const int *done, cudaStream_t st)
+{
+    const unsigned g = grid_for(n);
+    k_update<<<g, kThreads, sizeof(double2) * (nvec > 0 ? nvec : 0), st>>>(V, nvec, n, r, vcur, alpha, coef,
+                                                                        scratch, done);
+    k_sum_partials_re<<<1, kThreads, 0, st>>>(scratch, g, norm2, done);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_shard_beta(int i, double tol, const double *norm2, double *beta, double *maxbeta, int *done,
+                              int *iters, cudaStream_t st)
+{
+    k_beta_total<<<1, 32, 0, st>>>(norm2, i, tol, beta, maxbeta, done, iters);
     return cudaGetLastError();
 }
 

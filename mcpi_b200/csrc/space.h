@@ -73,7 +73,11 @@ struct mcpi_space_s {
     int fused_lead = 128;
     bool fz_ready = false;
     mcpi::FusedPlan fz{};
-    int *d_fz = nullptr;             // one allocation: need | order | flags | ctl
+    int *d_fz = nullptr;             // one allocation: need | order | ctl | count
+    // mcpi_apply_h_rows: the (N-2)-configuration range its last row block reads
+    int64_t mr_r0 = -1, mr_r1 = -1;
+    uint32_t mr_lo = 0, mr_hi = 0;
+    uint32_t *d_mr = nullptr;
     // grow-only workspaces kept between calls: Krylov basis of mcpi_ground,
     // state block and residual of mcpi_lanczos
     void *d_basis = nullptr, *d_lzblk = nullptr, *d_lzr = nullptr;

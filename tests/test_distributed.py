@@ -1,4 +1,4 @@
-"""Row-sharded Lanczos (mcpi_b200/distributed.py) with world size 2 on CPU (gloo).
+"""Row-sharded Lanczos (mcpi_b200/distributed.py) with world sizes 2 and 3 on CPU (gloo).
 
 The local operator is the oracle's row-range H.psi (the GPU path uses
 mcpi_apply_h_rows); what is tested is the sharding, the all-gathers and the
@@ -53,9 +53,12 @@ def _worker(rank, world, port, N, M, kind, lm, out_dir):
     dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("N,M,kind,lm", [(6, 7, "lieb", 40), (5, 5, "random", 30)])
-def test_sharded_lanczos_world2(tmp_path, orc, N, M, kind, lm):
-    world = 2
+@pytest.mark.parametrize("world,N,M,kind,lm", [(2, 6, 7, "lieb", 40), (2, 5, 5, "random", 30),
+                                               (3, 9, 5, "lieb", 40), (3, 10, 4, "random", 30)])
+def test_sharded_lanczos(tmp_path, orc, world, N, M, kind, lm):
+    # world 3: nc = 715 and 286 split into uneven row blocks (239/238/238, 96/95/95)
+    if world == 3:
+        assert orc.nc(N, M) % world != 0
     mp.start_processes(_worker, args=(world, _free_port(), N, M, kind, lm, str(tmp_path)), nprocs=world,
                        start_method="spawn")
     r = [dict(np.load(tmp_path / f"r{k}.npz")) for k in range(world)]

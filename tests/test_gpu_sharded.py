@@ -15,16 +15,25 @@ from conftest import rel
 pytestmark = pytest.mark.gpu
 
 
-def test_apply_h_rows_matches_full():
+@pytest.mark.parametrize("kind", ["random", "lieb"])
+def test_apply_h_rows_matches_full(kind):
+    # with Lieb integrals (momentum-block form) the pair-annihilation kernel runs
+    # only over the (N-2)-configurations the row block reads
     N, M = 9, 8
     C, Ho, Hint = mc.random_problem(N, M, 101)
+    if kind == "lieb":
+        Ho, Hint = mc.lieb_integrals(M, 2.5)
     sp = mc.FockSpace(N, M)
     sp.set_integrals(Ho, Hint)
     full = sp.apply_h(C).cpu().numpy()
     nc = sp.nc
-    for r0, r1 in [(0, nc), (0, 1), (nc - 1, nc), (123, 4567), (nc // 3, nc // 3 + 257), (5, 5)]:
+    for r0, r1 in [(0, nc), (0, 1), (nc - 1, nc), (123, 4567), (nc // 3, nc // 3 + 257), (5, 5),
+                   (nc // 2, nc), (0, nc // 8), (nc // 8, 2 * nc // 8), (7 * nc // 8, nc)]:
         part = sp.apply_h_rows(C, r0, r1).cpu().numpy()
         assert np.array_equal(part, full[r0:r1])        # same kernels, same arithmetic
+    for r0, r1 in [(0, nc // 8), (nc // 8, 2 * nc // 8), (0, nc // 8)]:   # the cached range, and a new one
+        C2 = np.roll(C, r0 + 1)
+        assert np.array_equal(sp.apply_h_rows(C2, r0, r1).cpu().numpy(), sp.apply_h(C2).cpu().numpy()[r0:r1])
 
 
 def test_sharded_lanczos_nccl_one_rank():
@@ -40,6 +49,11 @@ def test_sharded_lanczos_nccl_one_rank():
         sp.set_integrals(*mc.lieb_integrals(M, 5.0))
         C0 = torch.from_numpy(mc.random_problem(N, M, 102)[0]).cuda()
         sl = ShardedLanczos(sp.nc, lambda v: sp.apply_h_rows(v, sl.r0, sl.r1), torch.device("cuda"))
+        # one rank runs the same kernels in the same order as mcpi_lanczos: bit for bit
+        it, alpha, beta, _ = sl.lanczos(C0[sl.r0:sl.r1].clone(), 80)
+        it1, alpha1, beta1, _ = sp.lanczos(C0, 80)
+        assert it == it1 == 80
+        assert np.array_equal(alpha, alpha1) and np.array_equal(beta[:79], beta1[:79])
         E, psi, it = sl.ground(C0[sl.r0:sl.r1].clone(), 80)
         E1, psi1, it1 = sp.ground(C0, 80)
         assert it == it1 and abs(E - E1) <= 1e-10 * abs(E1)
