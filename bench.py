@@ -214,6 +214,7 @@ def run_batch(mc, torch, device, iters=120):
     t_batch = time.perf_counter() - t0
     arena = b.arena_bytes()
     tile, tune_ms = b.schedule()
+    hsched, hsched_ms = b.hpsi_schedule()
     b.close()
     spaces = []
     for k, (n, m, g) in enumerate(members):
@@ -236,7 +237,8 @@ def run_batch(mc, torch, device, iters=120):
             "sequential_seconds": t_seq, "speedup_vs_sequential": t_seq / t_batch,
             "max_rel_dE0_vs_sequential": dE, "steps_done_min": int(it.min()),
             "nc_min": min(ncs), "nc_max": max(ncs), "arena_gb": arena / 1e9,
-            "tile_rows": tile, "tile_probe_ms": {str(t): float(x) for t, x in zip((512, 1024, 2048), tune_ms)}}
+            "tile_rows": tile, "tile_probe_ms": {str(t): float(x) for t, x in zip((512, 1024, 2048), tune_ms)},
+            "hpsi_schedule": hsched, "hpsi_schedule_probe_ms": [float(x) for x in hsched_ms]}
 
 
 def run_sharded(mc, torch, dev, local, world, rank, barrier, max_over_ranks, iters=LANCZOS_ITERS):

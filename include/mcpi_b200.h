@@ -288,6 +288,17 @@ MCPI_API int mcpi_batch_set_schedule(mcpi_batch b, int tile_rows);
 /* The tile in use (0 before the first run) and, when it was autotuned, the
  * probe time of each candidate 512 / 1024 / 2048 in h_ms[0..2] (ms; may be NULL). */
 MCPI_API int mcpi_batch_schedule(mcpi_batch b, int *tile_rows, float *h_ms);
+/* Schedule of the batched H.psi: bit 0 runs the groups of members with the
+ * same M as concurrent graph branches (else one after another), bit 1 hands
+ * out their blocks interleaved across members (else member by member). -1
+ * (the default) lets the first mcpi_batch_run time one batched H.psi under
+ * each of the four schedules on this batch's own arena and keep the fastest;
+ * no schedule changes any member's arithmetic. Only before the first run. No
+ * reference counterpart. */
+MCPI_API int mcpi_batch_set_hpsi_schedule(mcpi_batch b, int schedule);
+/* The H.psi schedule in use (-1 before the first run) and the probe time of
+ * each schedule 0..3 in h_ms[0..3] when it was autotuned (ms; may be NULL). */
+MCPI_API int mcpi_batch_hpsi_schedule(mcpi_batch b, int *schedule, float *h_ms);
 MCPI_API int mcpi_batch_destroy(mcpi_batch b);
 
 /* ---- model inputs ------------------------------------------------------------ */

@@ -107,6 +107,8 @@ def lib():
         "mcpi_batch_arena_bytes": (i, [_vp, ct.POINTER(ct.c_size_t)]),
         "mcpi_batch_set_schedule": (i, [_vp, i]),
         "mcpi_batch_schedule": (i, [_vp, ct.POINTER(ct.c_int), _vp]),
+        "mcpi_batch_set_hpsi_schedule": (i, [_vp, i]),
+        "mcpi_batch_hpsi_schedule": (i, [_vp, ct.POINTER(ct.c_int), _vp]),
         "mcpi_batch_destroy": (i, [_vp]),
     }
     for name, (res, args) in sig.items():
@@ -462,6 +464,19 @@ class Batch:
         t = ct.c_int(0)
         ms = np.zeros(3, np.float32)
         _check(lib().mcpi_batch_schedule(self._h, ct.byref(t), _np_ptr(ms)))
+        return t.value, ms
+
+    def set_hpsi_schedule(self, schedule: int):
+        """Pin the batched H.psi schedule (0..3: bit 0 concurrent M groups, bit 1
+        interleaved blocks) or -1 to autotune at the first run."""
+        _check(lib().mcpi_batch_set_hpsi_schedule(self._h, int(schedule)))
+
+    def hpsi_schedule(self):
+        """(H.psi schedule in use or -1 before the first run, probe ms of
+        schedules 0..3 when autotuned, else zeros)."""
+        t = ct.c_int(0)
+        ms = np.zeros(4, np.float32)
+        _check(lib().mcpi_batch_hpsi_schedule(self._h, ct.byref(t), _np_ptr(ms)))
         return t.value, ms
 
     def close(self):

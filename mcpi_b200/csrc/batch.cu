@@ -49,6 +49,7 @@ constexpr int kThreads = 256;
 // rows per work tile of the vector stages: the autotuner picks one of these
 constexpr int kTileCands[3] = {512, 1024, 2048};
 constexpr int kTileMin = 512;
+constexpr int kUpdBatch = 8;   // basis entries in flight per thread in kb_update
 
 __device__ __forceinline__ double2 warp_sum2(double2 v)
 {
@@ -167,13 +168,14 @@ __global__ void __launch_bounds__(kThreads) kb_multidot(BatchLz *L, const int2 *
     }
 }
 
-// coef[j] = sum over tiles (one block per member, one warp per j)
+// coef[j] = sum over tiles (block (member, group of 8 j), one warp per j)
 __global__ void kb_coef(BatchLz *L, int nvec)
 {
     BatchLz &b = L[blockIdx.x];
     if (*b.done) return;
     const int wid = threadIdx.x / 32, lane = threadIdx.x % 32;
-    for (int j = wid; j < nvec; j += kThreads / 32) {
+    const int j = blockIdx.y * (kThreads / 32) + wid;
+    if (j < nvec) {
         double2 acc = make_double2(0.0, 0.0);
         for (int t = lane; t < b.ntiles; t += 32) {
             acc.x += b.part[(size_t)j * b.ntiles + t].x;
@@ -203,7 +205,20 @@ __global__ void __launch_bounds__(kThreads) kb_update(BatchLz *L, const int2 *__
     for (int64_t x = r0 + threadIdx.x; x < r1; x += kThreads) {
         const double2 y = b.r[x], v = vc[x];
         double2 u = make_double2(y.x - (a.x * v.x - a.y * v.y), y.y - (a.x * v.y + a.y * v.x));
-        for (int j = 0; j < nvec; ++j) {
+        // kUpdBatch basis entries loaded together, then subtracted in order j
+        int j = 0;
+        for (; j + kUpdBatch <= nvec; j += kUpdBatch) {
+            double2 p[kUpdBatch];
+#pragma unroll
+            for (int q = 0; q < kUpdBatch; ++q) p[q] = b.V[(size_t)(j + q) * b.nc + x];
+#pragma unroll
+            for (int q = 0; q < kUpdBatch; ++q) {
+                const double2 c = cs[j + q];
+                u.x -= p[q].x * c.x - p[q].y * c.y;
+                u.y -= p[q].x * c.y + p[q].y * c.x;
+            }
+        }
+        for (; j < nvec; ++j) {
             const double2 p = b.V[(size_t)j * b.nc + x], c = cs[j];
             u.x -= p.x * c.x - p.y * c.y;
             u.y -= p.x * c.y + p.y * c.x;
@@ -315,11 +330,20 @@ struct mcpi_batch_s {
     float tune_ms[3] = {0.f, 0.f, 0.f};   // probe time of each candidate tile
     struct Group {
         int M;
-        int2 *w1, *w2;
+        int2 *w1, *w2;     // member-major work tables
+        int2 *w1i, *w2i;   // the same blocks interleaved across members (round robin)
         int n1, n2;
         size_t sm1, sm2;
     };
     std::vector<Group> groups;
+    // batched H.psi schedule (the autotuner's second dimension): bit 0 = the
+    // M groups run as concurrent graph branches (else one after another),
+    // bit 1 = interleaved work tables (else member-major); -1 = autotune
+    int hsched = -1;
+    float hsched_ms[4] = {0.f, 0.f, 0.f, 0.f};
+    std::vector<cudaStream_t> side;    // one per group after the first
+    cudaEvent_t ev_fork = nullptr;
+    std::vector<cudaEvent_t> ev_join;
     double *d_E0 = nullptr;
     int *d_iters = nullptr;
     std::vector<char> ready;
@@ -420,20 +444,31 @@ int mcpi_batch_create(int count, const int *N, const int *M, int lm, int device,
     std::vector<int> Ms(M, M + count);
     std::sort(Ms.begin(), Ms.end());
     Ms.erase(std::unique(Ms.begin(), Ms.end()), Ms.end());
-    std::vector<std::vector<int2>> w1(Ms.size()), w2(Ms.size());
+    std::vector<std::vector<int2>> w1(Ms.size()), w2(Ms.size()), w1i(Ms.size()), w2i(Ms.size());
     const int rpb1 = mcpi::batch_rows_per_block(1), rpb2 = mcpi::batch_rows_per_block(2);
-    for (size_t g = 0; g < Ms.size(); ++g)
+    for (size_t g = 0; g < Ms.size(); ++g) {
+        int64_t most1 = 0, most2 = 0;
         for (int m = 0; m < count; ++m) {
             if (M[m] != Ms[g]) continue;
             const mcpi_space_s *s = b->spaces[m];
-            for (int64_t k = 0; k < (s->nc2 + rpb1 - 1) / rpb1; ++k) w1[g].push_back(make_int2(m, (int)k));
-            for (int64_t k = 0; k < (s->nc + rpb2 - 1) / rpb2; ++k) w2[g].push_back(make_int2(m, (int)k));
+            const int64_t b1 = (s->nc2 + rpb1 - 1) / rpb1, b2 = (s->nc + rpb2 - 1) / rpb2;
+            for (int64_t k = 0; k < b1; ++k) w1[g].push_back(make_int2(m, (int)k));
+            for (int64_t k = 0; k < b2; ++k) w2[g].push_back(make_int2(m, (int)k));
+            most1 = std::max(most1, b1);
+            most2 = std::max(most2, b2);
         }
+        for (int64_t k = 0; k < most1; ++k)
+            for (int m = 0; m < count; ++m)
+                if (M[m] == Ms[g] && k < (b->spaces[m]->nc2 + rpb1 - 1) / rpb1) w1i[g].push_back(make_int2(m, (int)k));
+        for (int64_t k = 0; k < most2; ++k)
+            for (int m = 0; m < count; ++m)
+                if (M[m] == Ms[g] && k < (b->spaces[m]->nc + rpb2 - 1) / rpb2) w2i[g].push_back(make_int2(m, (int)k));
+    }
     size_t mbytes = mcpi::up256(sizeof(BatchLz) * count) + mcpi::up256(sizeof(BatchMember) * count) +
                     mcpi::up256(sizeof(int2) * vwork.size()) + mcpi::up256(sizeof(double) * count) +
                     mcpi::up256(sizeof(int) * count);
     for (size_t g = 0; g < Ms.size(); ++g)
-        mbytes += mcpi::up256(sizeof(int2) * w1[g].size()) + mcpi::up256(sizeof(int2) * w2[g].size());
+        mbytes += 2 * (mcpi::up256(sizeof(int2) * w1[g].size()) + mcpi::up256(sizeof(int2) * w2[g].size()));
     if (cudaMalloc(&b->meta, mbytes) != cudaSuccess) return cleanup(MCPI_ERR_NOMEM, "metadata allocation failed");
     char *p = b->meta;
     auto take = [&](size_t bytes) {
@@ -455,6 +490,8 @@ int mcpi_batch_create(int count, const int *N, const int *M, int lm, int device,
         G.M = Ms[g];
         G.w1 = reinterpret_cast<int2 *>(take(sizeof(int2) * w1[g].size()));
         G.w2 = reinterpret_cast<int2 *>(take(sizeof(int2) * w2[g].size()));
+        G.w1i = reinterpret_cast<int2 *>(take(sizeof(int2) * w1i[g].size()));
+        G.w2i = reinterpret_cast<int2 *>(take(sizeof(int2) * w2i[g].size()));
         G.n1 = (int)w1[g].size();
         G.n2 = (int)w2[g].size();
         int maxN = 0;
@@ -473,7 +510,19 @@ int mcpi_batch_create(int count, const int *N, const int *M, int lm, int device,
         if (e != cudaSuccess) break;
         e = cudaMemcpy(G.w1, w1[g].data(), sizeof(int2) * w1[g].size(), cudaMemcpyHostToDevice);
         if (e == cudaSuccess) e = cudaMemcpy(G.w2, w2[g].data(), sizeof(int2) * w2[g].size(), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(G.w1i, w1i[g].data(), sizeof(int2) * w1i[g].size(), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(G.w2i, w2i[g].data(), sizeof(int2) * w2i[g].size(), cudaMemcpyHostToDevice);
         b->groups.push_back(G);
+    }
+    // side streams and events for the concurrent H.psi schedule
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming);
+    for (size_t g = 1; g < b->groups.size() && e == cudaSuccess; ++g) {
+        cudaStream_t x = nullptr;
+        cudaEvent_t y = nullptr;
+        e = cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking);
+        if (e == cudaSuccess) b->side.push_back(x);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&y, cudaEventDisableTiming);
+        if (e == cudaSuccess) b->ev_join.push_back(y);
     }
     if (e != cudaSuccess) return cleanup(MCPI_ERR_CUDA, std::string("upload: ") + cudaGetErrorString(e));
     *out = b;
@@ -538,6 +587,33 @@ static cudaError_t set_tile(mcpi_batch b, int T)
     return e;
 }
 
+// One batched H.psi of Krylov vector vec under H.psi schedule sched (bits as
+// mcpi_batch_s::hsched): the M groups one after another on the batch's
+// stream, or as concurrent branches (side streams forked from and joined back
+// into it -- graph branches under capture).
+static cudaError_t enqueue_hpsi(mcpi_batch b, int vec, int sched)
+{
+    cudaStream_t st = b->stream;
+    const bool branches = (sched & 1) && b->groups.size() > 1, inter = (sched & 2) != 0;
+    cudaError_t e = cudaSuccess;
+    if (branches) {
+        e = cudaEventRecord(b->ev_fork, st);
+        for (size_t g = 1; g < b->groups.size() && e == cudaSuccess; ++g)
+            e = cudaStreamWaitEvent(b->side[g - 1], b->ev_fork, 0);
+    }
+    for (size_t g = 0; g < b->groups.size() && e == cudaSuccess; ++g) {
+        const auto &G = b->groups[g];
+        cudaStream_t s = branches && g > 0 ? b->side[g - 1] : st;
+        e = mcpi::launch_batch_apply_h(G.M, b->d_mem, inter ? G.w1i : G.w1, G.n1, G.sm1, inter ? G.w2i : G.w2, G.n2,
+                                       G.sm2, vec, s);
+        if (e == cudaSuccess && branches && g > 0) e = cudaEventRecord(b->ev_join[g - 1], s);
+    }
+    if (branches)
+        for (size_t g = 1; g < b->groups.size() && e == cudaSuccess; ++g)
+            e = cudaStreamWaitEvent(st, b->ev_join[g - 1], 0);
+    return e;
+}
+
 template <int T>
 static cudaError_t enqueue_solve_t(mcpi_batch b)
 {
@@ -548,14 +624,7 @@ static cudaError_t enqueue_solve_t(mcpi_batch b)
         e = cudaMemcpyAsync(b->lz[m].V, b->start[m], sizeof(double2) * b->lz[m].nc, cudaMemcpyDeviceToDevice, st);
     if (e != cudaSuccess) return e;
     mcpi::kb_reset<<<(nm + 127) / 128, 128, 0, st>>>(b->d_lz, nm, lm);
-    auto hpsi = [&](int vec) {
-        for (auto &G : b->groups) {
-            cudaError_t x = mcpi::launch_batch_apply_h(G.M, b->d_mem, G.w1, G.n1, G.sm1, G.w2, G.n2, G.sm2,
-                                                       vec, st);
-            if (x != cudaSuccess) return x;
-        }
-        return cudaSuccess;
-    };
+    auto hpsi = [&](int vec) { return enqueue_hpsi(b, vec, b->hsched); };
     const int nw = b->nvwork;
     e = hpsi(0);
     if (e != cudaSuccess) return e;
@@ -570,7 +639,7 @@ static cudaError_t enqueue_solve_t(mcpi_batch b)
         mcpi::kb_axpy_dot<T><<<nw, mcpi::kThreads, 0, st>>>(b->d_lz, b->d_vwork, i);
         mcpi::kb_sum_alpha<<<nm, mcpi::kThreads, 0, st>>>(b->d_lz, i + 1);
         mcpi::kb_multidot<T><<<nw, mcpi::kThreads, 0, st>>>(b->d_lz, b->d_vwork, i + 1, i + 2);
-        mcpi::kb_coef<<<nm, mcpi::kThreads, 0, st>>>(b->d_lz, i + 2);
+        mcpi::kb_coef<<<dim3(nm, (i + 2 + 7) / 8), mcpi::kThreads, 0, st>>>(b->d_lz, i + 2);
         mcpi::kb_update<T><<<nw, mcpi::kThreads, sizeof(double2) * (i + 2), st>>>(b->d_lz, b->d_vwork, i + 1,
                                                                                     i + 2);
     }
@@ -638,6 +707,39 @@ static cudaError_t autotune(mcpi_batch b)
     return e;
 }
 
+// The autotuner's H.psi dimension: one batched H.psi of the start vectors
+// under each schedule (CUDA events, best of three after a warm-up); keeps the
+// fastest. The schedule does not change any member's arithmetic.
+static cudaError_t autotune_hpsi(mcpi_batch b)
+{
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaError_t e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    for (int m = 0; m < b->count && e == cudaSuccess; ++m)
+        e = cudaMemcpyAsync(b->lz[m].V, b->start[m], sizeof(double2) * b->lz[m].nc, cudaMemcpyDeviceToDevice,
+                            b->stream);
+    if (e == cudaSuccess) mcpi::kb_reset<<<(b->count + 127) / 128, 128, 0, b->stream>>>(b->d_lz, b->count, b->lm);
+    int best = -1;
+    for (int c = 0; c < 4 && e == cudaSuccess; ++c) {
+        float ms = 1e30f;
+        for (int rep = 0; rep < 4 && e == cudaSuccess; ++rep) {
+            e = cudaEventRecord(e0, b->stream);
+            if (e == cudaSuccess) e = enqueue_hpsi(b, 0, c);
+            if (e == cudaSuccess) e = cudaEventRecord(e1, b->stream);
+            if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+            float t = 0.f;
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&t, e0, e1);
+            if (rep > 0 && t < ms) ms = t;
+        }
+        b->hsched_ms[c] = ms;
+        if (best < 0 || ms < b->hsched_ms[best]) best = c;
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (e == cudaSuccess) b->hsched = best;
+    return e;
+}
+
 extern "C" {
 
 int mcpi_batch_set_schedule(mcpi_batch b, int tile_rows)
@@ -648,6 +750,25 @@ int mcpi_batch_set_schedule(mcpi_batch b, int tile_rows)
         return bfail(MCPI_ERR_ARG, "mcpi_batch_set_schedule: tile_rows must be 0, 512, 1024 or 2048");
     b->tile = tile_rows;
     b->tuned = false;
+    return MCPI_OK;
+}
+
+int mcpi_batch_set_hpsi_schedule(mcpi_batch b, int schedule)
+{
+    if (!b) return bfail(MCPI_ERR_ARG, "null batch");
+    if (b->exec) return bfail(MCPI_ERR_STATE, "mcpi_batch_set_hpsi_schedule: the solve has already been captured");
+    if (schedule < -1 || schedule > 3) return bfail(MCPI_ERR_ARG, "mcpi_batch_set_hpsi_schedule: schedule must be -1 .. 3");
+    b->hsched = schedule;
+    for (float &x : b->hsched_ms) x = 0.f;
+    return MCPI_OK;
+}
+
+int mcpi_batch_hpsi_schedule(mcpi_batch b, int *schedule, float *h_ms)
+{
+    if (!b) return bfail(MCPI_ERR_ARG, "null batch");
+    if (schedule) *schedule = b->exec ? b->hsched : -1;
+    if (h_ms)
+        for (int c = 0; c < 4; ++c) h_ms[c] = b->hsched_ms[c];
     return MCPI_OK;
 }
 
@@ -669,6 +790,7 @@ int mcpi_batch_run(mcpi_batch b, double *h_E0, int *h_iters)
     cudaError_t e = cudaSuccess;
     if (!b->exec) {
         e = b->tile == 0 ? autotune(b) : set_tile(b, b->tile);
+        if (e == cudaSuccess && b->hsched < 0) e = autotune_hpsi(b);
         if (e != cudaSuccess) return bfail(MCPI_ERR_CUDA, std::string("batch schedule: ") + cudaGetErrorString(e));
         e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
         if (e == cudaSuccess) {
@@ -706,6 +828,9 @@ int mcpi_batch_destroy(mcpi_batch b)
     for (mcpi_space s : b->spaces) mcpi_space_destroy(s);
     cudaFree(b->arena);
     cudaFree(b->meta);
+    for (cudaStream_t x : b->side) cudaStreamDestroy(x);
+    for (cudaEvent_t x : b->ev_join) cudaEventDestroy(x);
+    if (b->ev_fork) cudaEventDestroy(b->ev_fork);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
     return MCPI_OK;

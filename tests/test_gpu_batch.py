@@ -93,3 +93,34 @@ def test_batch_schedules_agree():
         for k in range(len(members)):
             assert abs(E[k] - ref[k]) <= 1e-10 * max(1.0, abs(ref[k])), (tile, k, E[k], ref[k])
         b.close()
+
+
+def test_batch_hpsi_schedules_agree():
+    # the four batched H.psi schedules (concurrent M groups or not, interleaved
+    # blocks or not) change no member's arithmetic: bitwise equal results
+    members = [(6, 7), (8, 9), (5, 11), (9, 7), (7, 11)]
+    gs = [0.3, 2.0, 30.0, 0.7, 5.0]
+    lm = 30
+    results = []
+    for sched in range(4):
+        b = mc.Batch(members, lm)
+        b.set_schedule(1024)
+        b.set_hpsi_schedule(sched)
+        for k, ((N, M), g) in enumerate(zip(members, gs)):
+            b.set_integrals(k, *mc.lieb_integrals(M, g))
+            b.set_start(k, _start(b.nc[k], 200 + k))
+        results.append(b.run())
+        assert b.hpsi_schedule()[0] == sched
+        b.close()
+    for E, it in results[1:]:
+        assert np.array_equal(E, results[0][0]) and np.array_equal(it, results[0][1])
+    # autotuned: one of the four, with its probe times
+    b = mc.Batch(members, lm)
+    for k, ((N, M), g) in enumerate(zip(members, gs)):
+        b.set_integrals(k, *mc.lieb_integrals(M, g))
+        b.set_start(k, _start(b.nc[k], 200 + k))
+    E, it = b.run()
+    sched, ms = b.hpsi_schedule()
+    assert 0 <= sched <= 3 and np.all(ms > 0)
+    assert np.allclose(E, results[0][0], rtol=1e-10, atol=1e-10)
+    b.close()
