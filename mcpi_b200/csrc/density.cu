@@ -193,7 +193,7 @@ __global__ void __launch_bounds__(kThreads) k_gram(Space sp, SpaceTables tb,
 // configurations m (4 per MMA). The complex product takes three real ones
 // (Gauss): t1 += Ar Br, t2 += Ai Bi, t3 += (Ar - Ai)(Br + Bi), and at the end
 // Re G = t1 + t2, Im G = t3 - t1 + t2 (A = Dphi, conjugated by the signs).
-// One persistent block per SM, warp-specialised: 8 gather warps fill tiles of
+// One persistent block per SM, warp-specialised: gather warps fill tiles of
 // GM configurations (one decode per configuration, K scattered 16-byte loads
 // of each vector from L2, the factors c_b(m), real and imaginary parts into
 // separate row-major planes) into two stages; 8 product warps each own a
@@ -208,8 +208,6 @@ __global__ void __launch_bounds__(kThreads) k_gram(Space sp, SpaceTables tb,
 // consecutive configurations of one fragment load fall into distinct banks.
 // ---------------------------------------------------------------------------
 constexpr int kDmmaPW = 8;                            // product warps
-constexpr int kDmmaGW = 8;                            // gather warps
-constexpr int kDmmaThreads = (kDmmaPW + kDmmaGW) * 32;
 constexpr int kDmmaStages = 2;
 constexpr int kDmmaUnroll = 4;   // configuration steps of the product loop unrolled together
 constexpr int kDmmaMaxM = 12;        // rho2 of one state
@@ -230,7 +228,13 @@ struct DmmaGram {
     static constexpr int NP = SAME ? 2 : 6;
     static constexpr int GM = SAME ? 64 : 32;        // configurations per tile
     static constexpr int LD = GM + 4;                // plane row stride (doubles)
-    static constexpr int GT = kDmmaGW * 32;          // gather threads
+    // gather warps: 8 for one state up to M = 10 (four threads per
+    // configuration of a 64-configuration tile), else 4 (the transition form
+    // loads two vectors, and M > 10 has more accumulators: with 8 warps, 128
+    // registers per thread would spill)
+    static constexpr int GW = (SAME && M <= 10) ? 8 : 4;
+    static constexpr int THREADS = (kDmmaPW + GW) * 32;
+    static constexpr int GT = GW * 32;               // gather threads
     static constexpr int PARTS = GT / GM;            // gather threads per configuration
     static constexpr int ntiles()
     {
@@ -277,8 +281,71 @@ __device__ __forceinline__ void dmma_m16n8k4(double (&c)[4], double a0, double a
         : "d"(a0), "d"(a1), "d"(b));
 }
 
+// One gather thread's share of a tile: configuration m (tile column ml), the
+// pair columns col with col % PARTS == PART. All of its loads are issued
+// before any is consumed (the columns are compile-time constants, so the
+// loaded values stay in registers), then the scaled values and the Gauss sum
+// planes go to the stage's planes pl.
+template <int M, bool SAME, int PART>
+__device__ __forceinline__ void dmma_gather(const Space &sp, const SpaceTables &tb, const uint32_t *W,
+                                            const double *sq, const double2 *__restrict__ phi,
+                                            const double2 *__restrict__ psi, double *pl, uint32_t m, int ml)
+{
+    using D = DmmaGram<M, SAME>;
+    constexpr int K = D::K, KP = D::KP, LD = D::LD, PARTS = D::PARTS;
+    constexpr int NPP = (K + PARTS - 1 - PART) / PARTS;   // my columns
+    if (m >= sp.nc2) {
+#pragma unroll
+        for (int k = 0; k < NPP; ++k)
+#pragma unroll
+            for (int p = 0; p < D::NP; ++p) pl[(p * KP + PART + k * PARTS) * LD + ml] = 0.0;
+        return;
+    }
+    const int ws = sp.wstride;
+    int u[M], Q[M];
+    occupations<M>(tb.occ2, tb.occ_bits, m, sp.N - 2, sp.nc2, W, ws, u, Q);
+    uint32_t B0[M], B1[M], B2[M];
+    prefix_table<M>(Q, 0, W, ws, B0);
+    prefix_table<M>(Q, 1, W, ws, B1);
+    prefix_table<M>(Q, 2, W, ws, B2);
+    double2 x[NPP > 0 ? NPP : 1], y[SAME ? 1 : (NPP > 0 ? NPP : 1)];
+    {
+        int k = 0;
+#pragma unroll
+        for (int q = 0; q < M; ++q)
+#pragma unroll
+            for (int l = q; l < M; ++l)
+                if (pair_index(q, l, M) % PARTS == PART) {
+                    const uint32_t j = idx_add2(sp.nc, B0, B1, B2, q, l, M);
+                    x[k] = __ldg(phi + j);
+                    if constexpr (!SAME) y[k] = __ldg(psi + j);
+                    ++k;
+                }
+    }
+    int k = 0;
+#pragma unroll
+    for (int q = 0; q < M; ++q)
+#pragma unroll
+        for (int l = q; l < M; ++l)
+            if (pair_index(q, l, M) % PARTS == PART) {
+                const int col = pair_index(q, l, M);
+                const double c = (q == l) ? sq[u[q] + 1] * sq[u[q] + 2] : sq[u[q] + 1] * sq[u[l] + 1];
+                const double xr = c * x[k].x, xi = c * x[k].y;
+                pl[col * LD + ml] = xr;
+                pl[(KP + col) * LD + ml] = xi;
+                if constexpr (D::SUMS) {
+                    const double yr = c * y[k].x, yi = c * y[k].y;
+                    pl[(2 * KP + col) * LD + ml] = xr - xi;
+                    pl[(3 * KP + col) * LD + ml] = yr;
+                    pl[(4 * KP + col) * LD + ml] = yi;
+                    pl[(5 * KP + col) * LD + ml] = yr + yi;
+                }
+                ++k;
+            }
+}
+
 template <int M, bool SAME>
-__global__ void __launch_bounds__(kDmmaThreads, 1)
+__global__ void __launch_bounds__(DmmaGram<M, SAME>::THREADS, 1)
     k_gram_dmma(Space sp, SpaceTables tb, const double2 *__restrict__ phi, const double2 *__restrict__ psi,
                 double2 *__restrict__ partial, int *status, long long wait_cycles, int test_stall)
 {
@@ -324,38 +391,16 @@ __global__ void __launch_bounds__(kDmmaThreads, 1)
             }
             double *pl = planes + (size_t)st * D::NP * KP * LD;
             const uint32_t m = (blockIdx.x + it * gridDim.x) * GM + ml;
-            if (m < nh) {
-                int u[M], Q[M];
-                occupations<M>(tb.occ2, tb.occ_bits, m, sp.N - 2, nh, W, ws, u, Q);
-                uint32_t B0[M], B1[M], B2[M];
-                prefix_table<M>(Q, 0, W, ws, B0);
-                prefix_table<M>(Q, 1, W, ws, B1);
-                prefix_table<M>(Q, 2, W, ws, B2);
-#pragma unroll
-                for (int q = 0; q < M; ++q)
-#pragma unroll
-                    for (int l = q; l < M; ++l) {
-                        const int col = pair_index(q, l, M);
-                        if (col % D::PARTS != part) continue;
-                        const uint32_t j = idx_add2(sp.nc, B0, B1, B2, q, l, M);
-                        const double c = (q == l) ? sq[u[q] + 1] * sq[u[q] + 2] : sq[u[q] + 1] * sq[u[l] + 1];
-                        const double2 x = __ldg(phi + j);
-                        const double xr = c * x.x, xi = c * x.y;
-                        pl[col * LD + ml] = xr;
-                        pl[(KP + col) * LD + ml] = xi;
-                        if constexpr (D::SUMS) {
-                            const double2 y = __ldg(psi + j);
-                            const double yr = c * y.x, yi = c * y.y;
-                            pl[(2 * KP + col) * LD + ml] = xr - xi;
-                            pl[(3 * KP + col) * LD + ml] = yr;
-                            pl[(4 * KP + col) * LD + ml] = yi;
-                            pl[(5 * KP + col) * LD + ml] = yr + yi;
-                        }
-                    }
-            } else {
-                for (int col = part; col < K; col += D::PARTS)
-#pragma unroll
-                    for (int p = 0; p < D::NP; ++p) pl[(p * KP + col) * LD + ml] = 0.0;
+            switch (part) {   // the part as a template argument: its pair columns are compile-time constants
+            case 0: dmma_gather<M, SAME, 0>(sp, tb, W, sq, phi, psi, pl, m, ml); break;
+            case 1: dmma_gather<M, SAME, 1>(sp, tb, W, sq, phi, psi, pl, m, ml); break;
+            case 2: dmma_gather<M, SAME, 2>(sp, tb, W, sq, phi, psi, pl, m, ml); break;
+            case 3: dmma_gather<M, SAME, 3>(sp, tb, W, sq, phi, psi, pl, m, ml); break;
+            case 4: if constexpr (D::PARTS > 4) dmma_gather<M, SAME, 4>(sp, tb, W, sq, phi, psi, pl, m, ml); break;
+            case 5: if constexpr (D::PARTS > 5) dmma_gather<M, SAME, 5>(sp, tb, W, sq, phi, psi, pl, m, ml); break;
+            case 6: if constexpr (D::PARTS > 6) dmma_gather<M, SAME, 6>(sp, tb, W, sq, phi, psi, pl, m, ml); break;
+            case 7: if constexpr (D::PARTS > 7) dmma_gather<M, SAME, 7>(sp, tb, W, sq, phi, psi, pl, m, ml); break;
+            default: break;
             }
             mbar_arrive(full + st);
         }
@@ -604,7 +649,7 @@ cudaError_t density_m(const Space &sp, const SpaceTables &tb, const double2 *phi
             const size_t sm = Dm::smem(sp.wstride);
             cudaError_t e = cudaFuncSetAttribute(k_gram_dmma<M, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
             if (e != cudaSuccess) return e;
-            k_gram_dmma<M, true><<<gx, kDmmaThreads, sm, st>>>(sp, tb, phi, psi, partial, status, wait_cycles,
+            k_gram_dmma<M, true><<<gx, Dm::THREADS, sm, st>>>(sp, tb, phi, psi, partial, status, wait_cycles,
                                                                test_stall);
             k_gram_finish<M, 2, 2><<<(nout + 255) / 256, 256, 0, st>>>(partial, gx, out);
             return cudaGetLastError();
@@ -617,7 +662,7 @@ cudaError_t density_m(const Space &sp, const SpaceTables &tb, const double2 *phi
             const size_t sm = Dm::smem(sp.wstride);
             cudaError_t e = cudaFuncSetAttribute(k_gram_dmma<M, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
             if (e != cudaSuccess) return e;
-            k_gram_dmma<M, false><<<gx, kDmmaThreads, sm, st>>>(sp, tb, phi, psi, partial, status, wait_cycles,
+            k_gram_dmma<M, false><<<gx, Dm::THREADS, sm, st>>>(sp, tb, phi, psi, partial, status, wait_cycles,
                                                                 test_stall);
             k_gram_finish<M, 2, 0><<<(nout + 255) / 256, 256, 0, st>>>(partial, gx, out);
             return cudaGetLastError();
