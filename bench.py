@@ -350,13 +350,16 @@ def run_large(mc, torch, device):
     r2 = sp.rho2(psi)
     torch.cuda.synchronize()
 
-    def timed(f):
+    def timed(f, reps=10):
+        # back-to-back calls: the mean device time per call (the host's launch
+        # latency overlaps the previous call)
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record()
-        y = f(psi)
+        for _ in range(reps):
+            y = f(psi)
         b.record()
         b.synchronize()
-        return y, a.elapsed_time(b) * 1e-3
+        return y, a.elapsed_time(b) * 1e-3 / reps
 
     r1, t_r1 = timed(sp.rho1)
     r2, t_r2 = timed(sp.rho2)
@@ -422,10 +425,11 @@ def run_general(mc, torch, device):
             f(X[0])                                   # first call allocates its buffer
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record()
-            f(X[0])
+            for k in range(10):                       # back to back: mean device time per call
+                f(X[k % ROTATE])
             b.record()
             b.synchronize()
-            dens[name] = a.elapsed_time(b)
+            dens[name] = a.elapsed_time(b) / 10
         flops = 8.0 * P * P * nc2
         tf = flops / (k1 * 1e-3) / 1e12
         out[f"n{N}_m{M}"] = {"workload": f"random integrals N={N} M={M} (nc={sp.nc})", "hpsi_ms": ms,
