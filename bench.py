@@ -66,7 +66,7 @@ def parse():
     p.add_argument("--no-general", action="store_true")
     p.add_argument("--no-sharded", action="store_true")
     p.add_argument("--no-adjoint", action="store_true")
-    p.add_argument("--profile", choices=["batch", "lanczos", "density"], default=None,
+    p.add_argument("--profile", choices=["batch", "lanczos", "density", "fused"], default=None,
                    help="run only this section (for profiler launch lists), print its timings")
     return p.parse_args()
 
@@ -705,7 +705,8 @@ def run_profile(args):
     with the autotuner, then one replay); 'lanczos' = one 150-step ground state
     of the N=16, M=10 workload after a warm-up solve; 'density' = rho1, rho2
     and the transition rho2 of seeded N=16, M=10 states (--steps calls each
-    after --warmup, CUDA events)."""
+    after --warmup, CUDA events); 'fused' = H.psi of the N=16, M=10 workload
+    with the two kernels and with the fused kernel."""
     import torch
 
     import mcpi_b200 as mc
@@ -747,6 +748,39 @@ def run_profile(args):
             torch.cuda.synchronize()
             out[name + "_ms"] = a.elapsed_time(b) / args.steps
         sp.close()
+    elif args.profile == "fused":
+        # H.psi of the N=16, M=10 workload with the two kernels and with the
+        # fused kernel (MCPI_OPT_FUSED_HPSI; lead 192), --steps calls each on
+        # rotating states after --warmup; the results must agree bit for bit
+        gen = torch.Generator(device="cuda:0")
+        gen.manual_seed(1234)
+        X = None
+        out = {"section": "fused", "workload": f"Lieb-Liniger N={N_PART} M={M_ORB}"}
+        ref = None
+        for name, fused in (("two_kernels", 0), ("fused", 1)):
+            sp = mc.FockSpace(N_PART, M_ORB, device=0)
+            sp.set_option(mc.OPT_FUSED_HPSI, fused)
+            sp.set_option(mc.OPT_FUSED_LEAD, 192)
+            sp.set_integrals(*mc.lieb_integrals(M_ORB, G, L_RING))
+            if X is None:
+                X = torch.randn((ROTATE, sp.nc), dtype=torch.complex128, device=sp.torch_device, generator=gen)
+            y = sp.empty()
+            for w in range(args.warmup):
+                sp.apply_h(X[w % ROTATE], y)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            a.record()
+            for k in range(args.steps):
+                sp.apply_h(X[k % ROTATE], y)
+            b.record()
+            torch.cuda.synchronize()
+            out[name + "_ms"] = a.elapsed_time(b) / args.steps
+            z = sp.apply_h(X[0])
+            if ref is None:
+                ref = z
+            else:
+                out["bitwise_equal"] = bool(torch.equal(ref, z))
+            sp.close()
     else:
         sp = mc.FockSpace(N_PART, M_ORB, device=0)
         sp.set_integrals(*mc.lieb_integrals(M_ORB, G, L_RING))
