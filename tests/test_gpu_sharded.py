@@ -61,3 +61,69 @@ def test_sharded_lanczos_nccl_one_rank():
                    psi1.cpu().numpy()) < 1e-8
     finally:
         dist.destroy_process_group()
+
+
+def test_shard_primitives_three_virtual_ranks():
+    # three ranks with uneven row blocks emulated in one process on one GPU: each
+    # rank's shard of every step runs in the library's kernels (mcpi_shard_*,
+    # mcpi_apply_h_rows on the gathered vector), and the all-reduce is the sum of
+    # the ranks' device scalars -- the recurrence must match mcpi_lanczos
+    from mcpi_b200.distributed import DeviceShardOps, row_block
+    N, M, lm, W = 10, 8, 60, 3
+    sp = mc.FockSpace(N, M)
+    sp.set_integrals(*mc.lieb_integrals(M, 4.0))
+    nc = sp.nc
+    assert nc % W != 0
+    C0 = torch.from_numpy(mc.random_problem(N, M, 103)[0]).cuda()
+    blocks = [row_block(nc, W, r) for r in range(W)]
+    dev = torch.device("cuda")
+    ops = [DeviceShardOps(b - a, lm, dev) for a, b in blocks]
+    V = [torch.zeros((lm, b - a), dtype=torch.complex128, device=dev) for a, b in blocks]
+    for r, (a, b) in enumerate(blocks):
+        V[r][0] = C0[a:b]
+    alpha = [torch.zeros(lm, dtype=torch.complex128, device=dev) for _ in range(W)]
+    beta = torch.zeros(lm, dtype=torch.float64, device=dev)
+    coef = [torch.zeros(lm, dtype=torch.complex128, device=dev) for _ in range(W)]
+    norm2 = [torch.zeros(1, dtype=torch.float64, device=dev) for _ in range(W)]
+    maxb = torch.zeros(1, dtype=torch.float64, device=dev)
+    done = torch.zeros(1, dtype=torch.int32, device=dev)
+    iters = torch.full((1,), lm, dtype=torch.int32, device=dev)
+
+    def allsum(ts, sl):
+        tot = sum(t[sl] for t in ts)
+        for t in ts:
+            t[sl] = tot
+
+    def gather(i):
+        return torch.cat([V[r][i] for r in range(W)])
+
+    full = gather(0)
+    R = [sp.apply_h_rows(full, a, b) for a, b in blocks]
+    for r in range(W):
+        ops[r].axpy_dot(None, V[r][0], R[r], None, alpha[r][0:1], done)
+    allsum(alpha, slice(0, 1))
+    for r in range(W):
+        ops[r].update(None, 0, R[r], V[r][0], alpha[r][0:1], None, norm2[r], done)
+    allsum(norm2, slice(0, 1))
+    for i in range(lm - 1):
+        ops[0].beta(i, 1e-15, norm2[0], beta, maxb, done, iters)
+        for r in range(W):
+            ops[r].scale(R[r], V[r][i + 1], beta[i:i + 1], done)
+        full = gather(i + 1)
+        R = [sp.apply_h_rows(full, a, b) for a, b in blocks]
+        for r in range(W):
+            ops[r].axpy_dot(V[r][i], V[r][i + 1], R[r], beta[i:i + 1], alpha[r][i + 1:i + 2], done)
+        allsum(alpha, slice(i + 1, i + 2))
+        for r in range(W):
+            ops[r].multidot(V[r], i + 2, R[r], V[r][i + 1], alpha[r][i + 1:i + 2], coef[r], done)
+        allsum(coef, slice(0, i + 2))
+        for r in range(W):
+            ops[r].update(V[r], i + 2, R[r], V[r][i + 1], alpha[r][i + 1:i + 2], coef[r], norm2[r], done)
+        allsum(norm2, slice(0, 1))
+    it1, alpha1, beta1, _ = sp.lanczos(C0, lm)
+    assert int(iters[0]) == it1 == lm
+    a = alpha[0].cpu().numpy()
+    scale = np.abs(alpha1).max()
+    assert np.abs(a - alpha1).max() <= 1e-10 * scale
+    assert np.abs(beta.cpu().numpy()[: lm - 1] - beta1[: lm - 1]).max() <= 1e-10 * scale
+    sp.close()
