@@ -170,7 +170,8 @@ class ShardedLanczos:
         shards padded to the largest block)."""
         n = shard.numel()
         send[:n].copy_(shard)
-        dist.all_gather_into_tensor(gbuf, send, group=self.group)
+        # complex as (re, im) pairs: every backend gathers float64
+        dist.all_gather_into_tensor(torch.view_as_real(gbuf), torch.view_as_real(send), group=self.group)
         g = gbuf.view(self.world, self.maxb)
         if all(b - a == self.maxb for a, b in self.counts):
             return gbuf[: self.nc]
