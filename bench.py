@@ -66,7 +66,7 @@ def parse():
     p.add_argument("--no-general", action="store_true")
     p.add_argument("--no-sharded", action="store_true")
     p.add_argument("--no-adjoint", action="store_true")
-    p.add_argument("--profile", choices=["batch", "lanczos", "density", "fused"], default=None,
+    p.add_argument("--profile", choices=["batch", "lanczos", "density", "hpsi"], default=None,
                    help="run only this section (for profiler launch lists), print its timings")
     return p.parse_args()
 
@@ -705,8 +705,8 @@ def run_profile(args):
     with the autotuner, then one replay); 'lanczos' = one 150-step ground state
     of the N=16, M=10 workload after a warm-up solve; 'density' = rho1, rho2
     and the transition rho2 of seeded N=16, M=10 states (--steps calls each
-    after --warmup, CUDA events); 'fused' = H.psi of the N=16, M=10 workload
-    with the two kernels and with the fused kernel."""
+    after --warmup, CUDA events); 'hpsi' = H.psi of the N=16, M=10 workload
+    with the two pair kernels, the fused kernel and the direct kernel."""
     import torch
 
     import mcpi_b200 as mc
@@ -748,17 +748,20 @@ def run_profile(args):
             torch.cuda.synchronize()
             out[name + "_ms"] = a.elapsed_time(b) / args.steps
         sp.close()
-    elif args.profile == "fused":
-        # H.psi of the N=16, M=10 workload with the two kernels and with the
-        # fused kernel (MCPI_OPT_FUSED_HPSI; lead 192), --steps calls each on
-        # rotating states after --warmup; the results must agree bit for bit
+    elif args.profile == "hpsi":
+        # H.psi of the N=16, M=10 workload in its three forms: the two pair
+        # kernels, the fused kernel (MCPI_OPT_FUSED_HPSI; lead 192) and the
+        # direct kernel (MCPI_OPT_DIRECT_HPSI), --steps calls each on rotating
+        # states after --warmup. The fused form agrees with the two kernels bit
+        # for bit; the direct form sums in another order (relative difference)
         gen = torch.Generator(device="cuda:0")
         gen.manual_seed(1234)
         X = None
-        out = {"section": "fused", "workload": f"Lieb-Liniger N={N_PART} M={M_ORB}"}
+        out = {"section": "hpsi", "workload": f"Lieb-Liniger N={N_PART} M={M_ORB}"}
         ref = None
-        for name, fused in (("two_kernels", 0), ("fused", 1)):
+        for name, fused, direct in (("two_kernels", 0, 0), ("fused", 1, 0), ("direct", 0, 1)):
             sp = mc.FockSpace(N_PART, M_ORB, device=0)
+            sp.set_option(mc.OPT_DIRECT_HPSI, direct)
             sp.set_option(mc.OPT_FUSED_HPSI, fused)
             sp.set_option(mc.OPT_FUSED_LEAD, 192)
             sp.set_integrals(*mc.lieb_integrals(M_ORB, G, L_RING))
@@ -778,8 +781,10 @@ def run_profile(args):
             z = sp.apply_h(X[0])
             if ref is None:
                 ref = z
+            elif name == "fused":
+                out["fused_bitwise_equal"] = bool(torch.equal(ref, z))
             else:
-                out["bitwise_equal"] = bool(torch.equal(ref, z))
+                out["direct_rel_diff"] = float(torch.linalg.vector_norm(z - ref) / torch.linalg.vector_norm(ref))
             sp.close()
     else:
         sp = mc.FockSpace(N_PART, M_ORB, device=0)

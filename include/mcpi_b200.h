@@ -100,6 +100,12 @@ MCPI_API int mcpi_space_sync(mcpi_space sp);
  * configurations of the N-2 space each) the fused kernel's schedule runs
  * ahead of its consumers. */
 #define MCPI_OPT_FUSED_LEAD 9
+/* MCPI_OPT_DIRECT_HPSI: apply momentum-block integrals row by row, gathering
+ * every term straight from the state, with no P x NC(N-2,M) intermediate
+ * (whole-vector calls with N < 64; row ranges keep the two kernels).
+ * 0 off, 1 on, 2 (default) on for real block values and M <= 10, where
+ * it is the faster form. */
+#define MCPI_OPT_DIRECT_HPSI 11
 MCPI_API int mcpi_space_set_option(mcpi_space sp, int option, int value);
 MCPI_API int mcpi_space_dims(mcpi_space sp, int *N, int *M, int64_t *nc);
 /* Device memory on the space's device, and a synchronous copy in any direction
@@ -156,8 +162,8 @@ MCPI_API int mcpi_apply_h_rows(mcpi_space sp, const void *d_C, int64_t row0, int
 /* mcpi_apply_h, timed: runs it reps times with CUDA events around each of its
  * two kernels on the space's stream (synchronising after every repetition) and
  * returns their mean durations in ms: h_ms[0] pair annihilation + pair-matrix
- * kernel, h_ms[1] pair creation kernel (with MCPI_OPT_FUSED_HPSI on and
- * momentum-block integrals: h_ms[0] the fused kernel, h_ms[1] = 0). For
+ * kernel, h_ms[1] pair creation kernel (where the call takes the direct or
+ * the fused one-kernel form: h_ms[0] that kernel, h_ms[1] = 0). For
  * measurement, not for production. */
 MCPI_API int mcpi_apply_h_profile(mcpi_space sp, const void *d_C, void *d_out, int reps, float *h_ms);
 /* out = H C without allocating anything. No counterpart in the reference.

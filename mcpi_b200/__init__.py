@@ -41,6 +41,7 @@ OPT_TEST_STALL_GATHER = 6
 OPT_NO_OCC_TABLES = 7
 OPT_FUSED_HPSI = 8
 OPT_FUSED_LEAD = 9
+OPT_DIRECT_HPSI = 11
 
 
 class MCPIError(RuntimeError):

@@ -266,9 +266,14 @@ int reserve(void *&ptr, size_t &cap, size_t bytes)
 
 int ensure_fused(mcpi_space_s *sp);
 
-int ensure_E(mcpi_space_s *sp)
+PairOp op_view(const mcpi_space_s *sp, const DevPairOp &op);
+
+// The pair-space intermediate E (P x NC(N-2,M)) that the two-kernel and fused
+// forms of op pass between their halves; the direct form needs none.
+int ensure_E(mcpi_space_s *sp, const DevPairOp &op)
 {
     if (sp->N < 2) return MCPI_OK;
+    if (mcpi::hpsi_form(sp->sp, op_view(sp, op)) == mcpi::kFormDirect) return MCPI_OK;
     if (!sp->d_E) CK(cudaMalloc(&sp->d_E, sizeof(double2) * (size_t)sp->P * sp->nc2));
     return ensure_fused(sp);
 }
@@ -337,6 +342,7 @@ PairOp op_view(const mcpi_space_s *sp, const DevPairOp &op)
 {
     PairOp v = op.view();
     if (sp->fused_on && sp->fz_ready) v.fused = sp->fz;
+    v.direct = sp->direct_on;
     return v;
 }
 
@@ -359,7 +365,7 @@ int apply_op(mcpi_space_s *sp, const DevPairOp &op, const void *d_C, void *d_out
     if (!sp->has_op) return fail(MCPI_ERR_STATE, "mcpi_set_integrals has not been called");
     CHECK_ARG(d_C != d_out, "input and output must not alias");
     DeviceGuard g(sp->device);
-    int rc = ensure_E(sp);
+    int rc = ensure_E(sp, op);
     if (rc) return rc;
     CK(mcpi::launch_apply_h(sp->sp, sp->tables(), op_view(sp, op), op.blocks(), (const double2 *)d_C,
                             sp->d_E, (double2 *)d_out, sp->stream));
@@ -573,6 +579,10 @@ int mcpi_space_set_option(mcpi_space sp, int option, int value)
     case MCPI_OPT_FUSED_HPSI:
         if ((value != 0) != sp->fused_on) free_fused(sp);
         sp->fused_on = value != 0;
+        return MCPI_OK;
+    case MCPI_OPT_DIRECT_HPSI:
+        if (value < 0) return fail(MCPI_ERR_ARG, "direct form must be >= 0");
+        sp->direct_on = value;
         return MCPI_OK;
     case MCPI_OPT_FUSED_LEAD:
         if (value < 0) return fail(MCPI_ERR_ARG, "fused lead must be >= 0");
@@ -829,7 +839,7 @@ int mcpi_apply_h_host(mcpi_space sp, int count, const void *const *h_C, void *co
     if (!sp->has_op) return fail(MCPI_ERR_STATE, "mcpi_set_integrals has not been called");
     for (int k = 0; k < count; ++k) CHECK_ARG(h_C[k] && h_out[k], "mcpi_apply_h_host: null state pointer");
     DeviceGuard g(sp->device);
-    int rc = ensure_E(sp);
+    int rc = ensure_E(sp, sp->fwd);
     if (rc) return rc;
     const size_t bytes = sizeof(double2) * (size_t)sp->nc;
     if (!sp->host_pipe_ready) CK(make_host_pipe(sp, bytes));
@@ -859,15 +869,16 @@ int mcpi_apply_h_profile(mcpi_space sp, const void *d_C, void *d_out, int reps, 
     CHECK_ARG(sp && d_C && d_out && h_ms && reps >= 1, "mcpi_apply_h_profile: bad arguments");
     if (!sp->has_op) return fail(MCPI_ERR_STATE, "mcpi_set_integrals has not been called");
     DeviceGuard g(sp->device);
-    int rc = ensure_E(sp);
+    int rc = ensure_E(sp, sp->fwd);
     if (rc) return rc;
     cudaEvent_t ev[3];
     for (auto &e : ev) CK(cudaEventCreate(&e));
     float tot[2] = {0.f, 0.f};
     cudaError_t e = cudaSuccess;
     const PairOp fop = op_view(sp, sp->fwd);
-    if (fop.fused.order && sp->fwd.hblk) {
-        // fused form: one kernel, reported as h_ms[0]
+    const bool one = mcpi::hpsi_form(sp->sp, fop) != mcpi::kFormTwo;
+    if (one) {
+        // direct or fused form: one kernel, reported as h_ms[0]
         for (int r = 0; r < reps && e == cudaSuccess; ++r) {
             e = cudaEventRecord(ev[0], sp->stream);
             if (e == cudaSuccess)
@@ -880,7 +891,7 @@ int mcpi_apply_h_profile(mcpi_space sp, const void *d_C, void *d_out, int reps, 
             tot[0] += a;
         }
     }
-    for (int r = 0; r < reps && e == cudaSuccess && !(fop.fused.order && sp->fwd.hblk); ++r) {
+    for (int r = 0; r < reps && e == cudaSuccess && !one; ++r) {
         e = cudaEventRecord(ev[0], sp->stream);
         if (e == cudaSuccess)
             e = mcpi::launch_apply_h(sp->sp, sp->tables(), sp->fwd.view(), sp->fwd.blocks(),
@@ -914,13 +925,14 @@ int mcpi_apply_h_rows(mcpi_space sp, const void *d_C, int64_t row0, int64_t row1
     if (sp->N < 2 || sp->create_form != 0)
         return fail(MCPI_ERR_ARG, "row ranges need N >= 2 and the default pair-creation form");
     DeviceGuard g(sp->device);
-    int rc = ensure_E(sp);
+    int rc = ensure_E(sp, sp->fwd);
     if (rc) return rc;
     // kernel 1 only over the E columns these rows read (momentum-block form):
     // a rank of a sharded solve does not recompute the whole intermediate.
     // The range is found once per row block (one pass over its rows).
     uint32_t m0 = 0, m1 = 0xffffffffu;
-    if (sp->fwd.hblk && sp->M >= 2) {
+    const PairOp fop = op_view(sp, sp->fwd);
+    if (sp->fwd.hblk && sp->M >= 2 && mcpi::hpsi_form(sp->sp, fop) != mcpi::kFormDirect) {
         if (sp->mr_r0 != row0 || sp->mr_r1 != row1) {
             if (!sp->d_mr) CK(cudaMalloc(&sp->d_mr, 2 * sizeof(uint32_t)));
             uint32_t h[2];
@@ -936,7 +948,7 @@ int mcpi_apply_h_rows(mcpi_space sp, const void *d_C, int64_t row0, int64_t row1
         m0 = sp->mr_lo;
         m1 = sp->mr_hi + 1;
     }
-    CK(mcpi::launch_apply_h(sp->sp, sp->tables(), sp->fwd.view(), sp->fwd.blocks(), (const double2 *)d_C,
+    CK(mcpi::launch_apply_h(sp->sp, sp->tables(), fop, sp->fwd.blocks(), (const double2 *)d_C,
                             sp->d_E, (double2 *)d_out, sp->stream, 3, (uint32_t)row0, (uint32_t)row1, m0, m1));
     return MCPI_OK;
 }
@@ -1051,7 +1063,7 @@ int mcpi_lanczos(mcpi_space sp, void *d_lvec, int lm, double *h_diag, double *h_
     CHECK_ARG(sp && d_lvec && lm >= 1, "mcpi_lanczos: bad arguments");
     if (!sp->has_op) return fail(MCPI_ERR_STATE, "mcpi_set_integrals has not been called");
     DeviceGuard g(sp->device);
-    int rc = ensure_E(sp);
+    int rc = ensure_E(sp, sp->fwd);
     if (rc) return rc;
     const int64_t nc = sp->nc;
     const size_t npart = mcpi::lanczos_partial_elems(nc, lm);
@@ -1167,7 +1179,7 @@ int mcpi_ground_lowmem(mcpi_space sp, void *d_C, int niter, double *E0, int *ite
     CHECK_ARG(sp && d_C && E0 && niter >= 1 && niter <= 1 << 20, "mcpi_ground_lowmem: bad arguments");
     if (!sp->has_op) return fail(MCPI_ERR_STATE, "mcpi_set_integrals has not been called");
     DeviceGuard g(sp->device);
-    int rc = ensure_E(sp);
+    int rc = ensure_E(sp, sp->fwd);
     if (rc) return rc;
     const int64_t nc = sp->nc;
     const int lm = niter;

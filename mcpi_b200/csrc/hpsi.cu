@@ -987,6 +987,238 @@ __global__ void __launch_bounds__(kTC, 4) k_pair_create_smem(Space sp, SpaceTabl
 }
 
 // ---------------------------------------------------------------------------
+// Direct H.psi, momentum-block form: no intermediate. Written out per row,
+//   (H2 psi)(v) = sum_{a occupied in v} c_a(v) sum_{b in block(a)} Ht[a][b] c_b(v - a) psi[v - a + b],
+// the pair-space product with nothing stored between its two halves: every
+// term gathers straight from psi, which stays in L2 (32.7 MB at N=16, M=10),
+// so HBM carries only psi, out and the occupation table (about 82 MB against
+// the 1.5 GB of the two-kernel form with its P x NC(N-2,M) intermediate E).
+// Within a momentum block a = (k, s) and b = (q, l) have k + s = q + l, so
+// for b != a the orbitals q, l differ from k, s and one of two orders holds,
+// q < k <= s < l or k < q <= l < s. The prefix counts of v - a + b then move
+// by +1 on [q, k) and -1 on [s, l) (or -1 on [k, q) and +1 on [l, s)); with
+// per-row tables Dp[t] = sum_{i<t} W_i(P_i + 1) - W_i(P_i) and Dm (the same
+// with P_i - 1) the target index splits into a part of a and a part of b,
+//   q < k:  (base - Dp[k] + Dm[s]) + (Dp[q] - Dm[l])
+//   q > k:  (base + Dm[k] - Dp[s]) + (Dp[l] - Dm[q]),
+// formed once per block, so a term costs one addition for its index.
+// c_b(v - a) = sqrt((v_q+1)(v_l+1)) (sqrt((v_q+1)(v_q+2)) for q = l)
+// depends on v alone; the diagonal term b = a reads psi[v] with c_a(v)^2.
+// The gathers of R pairs of a block are issued together. REAL: the block
+// values are real (any real translation-invariant interaction), so a term is
+// a real coefficient times a complex gather -- two multiply-adds instead of
+// four, the same values. SMEM_D: the tables Dp, Dm sit in shared-memory
+// columns of their thread instead of registers.
+// ---------------------------------------------------------------------------
+template <int M, bool REAL, int R, bool SMEM_D>
+__global__ void __launch_bounds__(kTC, 3)
+    k_hpsi_direct(Space sp, SpaceTables tb, const __grid_constant__ MomBlocks<M> hp,
+                  const double2 *__restrict__ hdiag, const double2 *__restrict__ psi, double2 *__restrict__ out,
+                  uint32_t row0, uint32_t row1)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int ws = sp.wstride;
+    double2 *hd = reinterpret_cast<double2 *>(smem_raw);            // M
+    double *sqp = reinterpret_cast<double *>(hd + M);               // ws x ws: sqrt(x) sqrt(y)
+    uint32_t *W = reinterpret_cast<uint32_t *>(sqp + ws * ws);      // (M-1) x ws
+    uint32_t *FS = W + (M - 1) * ws, *GS = FS + M * kTC;            // SMEM_D: M x kTC each
+    for (int x = threadIdx.x; x < (M - 1) * ws; x += blockDim.x) W[x] = tb.W[x];
+    for (int x = threadIdx.x; x < ws * ws; x += blockDim.x) sqp[x] = tb.sq[x / ws] * tb.sq[x % ws];
+    if (threadIdx.x < M) hd[threadIdx.x] = hdiag[threadIdx.x];
+    __syncthreads();
+
+    const uint32_t i = row0 + blockIdx.x * kTC + threadIdx.x;   // rows [row0, row1) -> out[i - row0]
+    if (i >= row1) return;
+    int vv[M], P[M];
+    occupations<M>(tb.occ, tb.occ_bits, i, sp.N, sp.nc, W, ws, vv, P);
+    const double2 x0 = __ldg(psi + i);
+    double2 acc;
+    {
+        double2 h1 = make_double2(0.0, 0.0);
+#pragma unroll
+        for (int k = 0; k < M; ++k) {
+            h1.x += hd[k].x * vv[k];
+            h1.y += hd[k].y * vv[k];
+        }
+        acc = cmul(h1, x0);
+    }
+    // F[t] = sum_{i<t} W_i(P_i + 1) - W_i(P_i), G[t] the same with P_i - 1
+    uint32_t F[M], G[M], s0 = 0;
+    F[0] = G[0] = 0;
+#pragma unroll
+    for (int t = 1; t < M; ++t) {
+        const uint32_t w0 = W[(t - 1) * ws + P[t - 1]];
+        s0 += w0;
+        F[t] = F[t - 1] + (W[(t - 1) * ws + P[t - 1] + 1] - w0);
+        G[t] = G[t - 1] + (wlook(W, ws, t - 1, P[t - 1] - 1) - w0);
+    }
+    const uint32_t base = sp.nc - 1u - s0;
+    if constexpr (SMEM_D) {
+#pragma unroll
+        for (int t = 0; t < M; ++t) {
+            FS[t * kTC + threadIdx.x] = F[t];
+            GS[t * kTC + threadIdx.x] = G[t];
+        }
+    }
+    auto f = [&](int t) -> uint32_t { return SMEM_D ? FS[t * kTC + threadIdx.x] : F[t]; };
+    auto g = [&](int t) -> uint32_t { return SMEM_D ? GS[t * kTC + threadIdx.x] : G[t]; };
+    // occupations packed 6 bits each where they fit one word (fewer registers
+    // than the array; the launcher takes this form only for N < 64)
+    constexpr bool PACK = 6 * M <= 64;
+    uint64_t vw = 0;
+    if constexpr (PACK) {
+#pragma unroll
+        for (int o = 0; o < M; ++o) vw |= (uint64_t)vv[o] << (6 * o);
+    }
+    auto v = [&](int o) -> int { return PACK ? (int)((vw >> (6 * o)) & 63u) : vv[o]; };
+    constexpr int NB = M / 2 + 1;
+    int off = 0;
+#pragma unroll
+    for (int K = 0; K <= 2 * M - 2; ++K) {
+        const int qlo = K - (M - 1) > 0 ? K - (M - 1) : 0, qhi = K / 2, n = qhi - qlo + 1;
+        if (n == 1) {   // a single pair: only its diagonal term
+            const int k = qlo, s = K - k;
+            const double ca2 = k == s ? (double)(v(k) * (v(k) - 1)) : (double)(v(k) * v(s));
+            const double2 h = hp.v[off];
+            cfma(acc, make_double2(h.x * ca2, h.y * ca2), x0);
+            off += 1;
+            continue;
+        }
+        // per pair p = (q, l) of the block: its index parts YA = F[q] - G[l],
+        // YB = F[l] - G[q] (as a creation pair its X = base - Y) and its
+        // creation factor c_p(v - a) = sqrt(v_q + 1) sqrt(v_l + 1)
+        uint32_t YA[NB], YB[NB];
+        double cb[NB];
+#pragma unroll
+        for (int c = 0; c < NB; ++c)
+            if (c < n) {
+                const int q = qlo + c, l = K - q;
+                YA[c] = f(q) - g(l);
+                YB[c] = f(l) - g(q);
+                cb[c] = sqp[(v(q) + 1) * ws + (q == l ? v(q) + 2 : v(l) + 1)];
+            }
+#pragma unroll
+        for (int r0 = 0; r0 < NB; r0 += R)
+            if (r0 < n) {
+                double2 gv[R][NB];
+                double ca[R];
+#pragma unroll
+                for (int rr = 0; rr < R; ++rr) {
+                    const int r = r0 + rr;
+                    if (r < n) {
+                        const int k = qlo + r, s = K - k;
+                        // c_a(v) = sqrt(v_k) sqrt(v_s) (sqrt(v_k) sqrt(v_k - 1) for k = s): zero iff a is not in v
+                        ca[rr] = sqp[v(k) * ws + (k == s ? max(v(k) - 1, 0) : v(s))];
+                        const bool occ = ca[rr] != 0.0;
+                        const uint32_t XA = base - YA[r], XB = base - YB[r];
+#pragma unroll
+                        for (int c = 0; c < NB; ++c)
+                            if (c < n && c != r) {
+                                const uint32_t j = c < r ? XA + YA[c] : XB + YB[c];
+                                gv[rr][c] = occ ? __ldg(psi + j) : make_double2(0.0, 0.0);
+                            }
+                    }
+                }
+#pragma unroll
+                for (int rr = 0; rr < R; ++rr) {
+                    const int r = r0 + rr;
+                    if (r < n) {
+                        double2 e = make_double2(0.0, 0.0);
+#pragma unroll
+                        for (int c = 0; c < NB; ++c)
+                            if (c < n) {
+                                const double2 h = hp.v[off + r * n + c];
+                                const double w = c == r ? ca[rr] : cb[c];
+                                const double2 y = c == r ? x0 : gv[rr][c];
+                                if constexpr (REAL) {
+                                    const double t = h.x * w;
+                                    e.x = fma(t, y.x, e.x);
+                                    e.y = fma(t, y.y, e.y);
+                                } else {
+                                    cfma(e, make_double2(h.x * w, h.y * w), y);
+                                }
+                            }
+                        acc.x = fma(ca[rr], e.x, acc.x);
+                        acc.y = fma(ca[rr], e.y, acc.y);
+                    }
+                }
+            }
+        off += n * n;
+    }
+    out[i - row0] = acc;
+}
+
+template <int M, bool REAL, int R, bool SMEM_D>
+cudaError_t launch_direct(const Space &sp, const SpaceTables &tb, const MomBlocks<M> &hp, const double2 *hdiag,
+                          const double2 *psi, double2 *out, cudaStream_t st, uint32_t row0, uint32_t row1)
+{
+    const int ws = sp.wstride;
+    const size_t smem = sizeof(double2) * M + sizeof(double) * ws * ws + sizeof(uint32_t) * (M - 1) * ws +
+                        (SMEM_D ? 2 * sizeof(uint32_t) * M * kTC : 0);
+    if (smem > 48 * 1024) {
+        const cudaError_t e =
+            cudaFuncSetAttribute(k_hpsi_direct<M, REAL, R, SMEM_D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    const unsigned grid = (row1 - row0 + kTC - 1) / kTC;
+    k_hpsi_direct<M, REAL, R, SMEM_D><<<grid, kTC, smem, st>>>(sp, tb, hp, hdiag, psi, out, row0, row1);
+    return cudaGetLastError();
+}
+
+template <int M>
+cudaError_t direct_apply_m(const Space &sp, const SpaceTables &tb, const PairOp &op, const double2 *psi,
+                           double2 *out, cudaStream_t st, uint32_t row0, uint32_t row1)
+{
+    if (row1 <= row0) return cudaSuccess;
+    MomBlocks<M> hp;
+    bool real = true;
+    for (int x = 0; x < mom_values<M>(); ++x) {
+        hp.v[x] = op.hblk_host[x];
+        real = real && hp.v[x].y == 0.0;
+    }
+    const int form = op.direct;   // probe forms (3..6); 1 and 2 take the default
+    if (!real) {
+        if (form == 4) return launch_direct<M, false, 2, true>(sp, tb, hp, op.hdiag, psi, out, st, row0, row1);
+        return launch_direct<M, false, 1, true>(sp, tb, hp, op.hdiag, psi, out, st, row0, row1);
+    }
+    if (form == 3) return launch_direct<M, true, 1, true>(sp, tb, hp, op.hdiag, psi, out, st, row0, row1);
+    if (form == 5) return launch_direct<M, true, 1, false>(sp, tb, hp, op.hdiag, psi, out, st, row0, row1);
+    if (form == 6) return launch_direct<M, true, 2, false>(sp, tb, hp, op.hdiag, psi, out, st, row0, row1);
+    return launch_direct<M, true, 2, true>(sp, tb, hp, op.hdiag, psi, out, st, row0, row1);
+}
+
+}  // namespace
+
+// Number of momentum-block values for M orbitals, at run time.
+static int mom_count(int M)
+{
+    int s = 0;
+    for (int K = 0; K <= 2 * M - 2; ++K) {
+        const int qlo = K - (M - 1) > 0 ? K - (M - 1) : 0, n = K / 2 - qlo + 1;
+        s += n * n;
+    }
+    return s;
+}
+
+int hpsi_form(const Space &sp, const PairOp &op)
+{
+    if (sp.N < 2 || sp.M < 2 || !op.hblk_host || op.nhblk != mom_count(sp.M)) return kFormTwo;
+    if (op.direct && sp.N < 64 && op.create_form == 0) {
+        bool take = op.direct != 2;
+        if (!take && sp.M <= kDirectAutoMaxM) {   // default: real blocks of up to kDirectAutoMaxM orbitals
+            take = true;
+            for (int x = 0; x < op.nhblk && take; ++x) take = op.hblk_host[x].y == 0.0;
+        }
+        if (take) return kFormDirect;
+    }
+    if (op.fused.order && op.create_form == 0) return kFormFused;
+    return kFormTwo;
+}
+
+namespace {
+
+// ---------------------------------------------------------------------------
 // Fused H.psi, momentum-block form (FusedPlan in kernels.h). The two-kernel
 // path writes all of E (P x NC(N-2,M) complex, 719 MB at N=16, M=10) to HBM
 // and reads it back. Here one persistent grid walks kernel 1's tiles and
@@ -1303,9 +1535,12 @@ cudaError_t apply_h_m(const Space &sp, const SpaceTables &tb, const PairOp &op, 
     constexpr int P = M * (M + 1) / 2;
     const size_t tab = sizeof(double) * sp.wstride + sizeof(uint32_t) * (M - 1) * sp.wstride;
     if constexpr (M >= 2) {
-        if (sp.N >= 2 && stages == 3 && op.fused.order && op.hblk_host && op.nhblk == mom_values<M>() &&
-            row0 == 0 && row1 == sp.nc && op.create_form == 0)
-            return fused_apply_m<M>(sp, tb, op, psi, E, out, st);
+        if (stages == 3) {
+            const int form = hpsi_form(sp, op);
+            if (form == kFormDirect) return direct_apply_m<M>(sp, tb, op, psi, out, st, row0, row1);
+            if (form == kFormFused && row0 == 0 && row1 == sp.nc)
+                return fused_apply_m<M>(sp, tb, op, psi, E, out, st);
+        }
     }
     if (sp.N >= 2 && (stages & 1) && op.hblk) {
         // only the configurations [m0, m1) (a row block's range; the whole space by default)

@@ -59,7 +59,15 @@ struct PairOp {
     const double2 *hblk_host;
     // fused launch plan of the space (order == nullptr: two kernels)
     FusedPlan fused;
+    // direct form: momentum-block integrals applied row by row with no
+    // intermediate (0 off, 1 on, 2 on for real blocks and M <= kDirectAutoMaxM)
+    int direct;
 };
+
+// The form a whole-vector H.psi (both stages, all rows) takes with op.
+enum { kFormTwo = 0, kFormFused = 1, kFormDirect = 2 };
+constexpr int kDirectAutoMaxM = 10;
+int hpsi_form(const Space &sp, const PairOp &op);
 constexpr int kGemmMaxP = 78;   // M <= 12: Ht (zero-padded to a multiple of 8 rows) fits shared memory
 
 // Block-sparse form of the same pair matrix: when Ht decomposes into blocks

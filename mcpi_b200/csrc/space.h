@@ -31,7 +31,7 @@ struct DevPairOp {
     PairOp view() const
     {
         return PairOp{rowptr, col, val, hdiag, hfull, nnz, hblk, nhblk, create_form, status, hdense,
-                      wait_cycles, test_stall, hblk_h.empty() ? nullptr : hblk_h.data(), FusedPlan{}};
+                      wait_cycles, test_stall, hblk_h.empty() ? nullptr : hblk_h.data(), FusedPlan{}, 0};
     }
     BlockOp blocks() const { return BlockOp{prog, prog_bytes}; }
 };
@@ -70,6 +70,7 @@ struct mcpi_space_s {
     int create_form = 0;            // pair-creation kernel form (MCPI_OPT_CREATE_FORM)
     // fused H.psi (MCPI_OPT_FUSED_*): schedule built once per space by ensure_fused
     bool fused_on = false;
+    int direct_on = 2;               // MCPI_OPT_DIRECT_HPSI (default: real blocks, M <= 10)
     int fused_lead = 128;
     bool fz_ready = false;
     mcpi::FusedPlan fz{};

@@ -18,6 +18,7 @@ pytestmark = pytest.mark.gpu
 
 def _space(N, M, g, fused, lead=0):
     sp = mc.FockSpace(N, M)
+    sp.set_option(mc.OPT_DIRECT_HPSI, 0)       # the pair kernels, two or fused
     sp.set_option(mc.OPT_FUSED_HPSI, int(fused))
     sp.set_option(mc.OPT_FUSED_LEAD, lead)
     sp.set_integrals(*mc.lieb_integrals(M, g))

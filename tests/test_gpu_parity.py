@@ -263,8 +263,12 @@ def test_block_and_dense_pair_kernels_agree(orc, N, M, g):
     Ho, Hint = mc.lieb_integrals(M, g)
     C = mc.random_problem(N, M, 61)[0]
     sp = _space(N, M)
+    sp.set_option(mc.OPT_DIRECT_HPSI, 0)
     sp.set_integrals(Ho, Hint)
-    fast = sp.apply_h(C).cpu().numpy()                 # momentum-block kernel
+    fast = sp.apply_h(C).cpu().numpy()                 # momentum-block pair kernels
+    sp.set_option(mc.OPT_DIRECT_HPSI, 1)
+    direct = sp.apply_h(C).cpu().numpy()               # direct kernel
+    assert rel(direct, orc.apply_h(N, M, C, Ho, Hint, mode=2)) <= TOL
     sp.set_momentum_kernel(False)
     sp.set_integrals(Ho, Hint)
     blocks = sp.apply_h(C).cpu().numpy()               # generic block-sparse kernel
