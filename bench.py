@@ -181,6 +181,29 @@ def hpsi_bytes(nc, nc2, P):
     return {"pair_annihilate": 16 * nc + 16 * P * nc2, "pair_create": 16 * P * nc2 + 32 * nc}
 
 
+def direct_bytes(nc):
+    """Algorithmic HBM bytes per launch of the direct H.psi kernel: psi in, out,
+    and the 8-byte packed occupations of every row (the psi gathers are served
+    from L2: psi is 16 nc bytes, well under the 126 MB L2 at N=16, M=10)."""
+    return 16 * nc + 16 * nc + 8 * nc
+
+
+def mom_block_sizes(M):
+    """Pairs per momentum block K = k + s, K = 0 .. 2M-2."""
+    return [K // 2 - max(0, K - (M - 1)) + 1 for K in range(2 * M - 1)]
+
+
+def direct_gathers(M, nc2):
+    """psi gathers of one direct H.psi: every pair a of a block is in
+    NC(N-2,M) rows, each gathering the block's other n - 1 pairs."""
+    return nc2 * sum(n * (n - 1) for n in mom_block_sizes(M))
+
+
+def hpsi_terms(M, nc2):
+    """Terms (b, a) of one H.psi with momentum-block integrals, diagonal included."""
+    return nc2 * sum(n * n for n in mom_block_sizes(M))
+
+
 # ---------------------------------------------------------------------------
 # CPU baseline: oracle restatement of applyHconf_X on a row sample
 # ---------------------------------------------------------------------------
@@ -340,7 +363,8 @@ def run_large(mc, torch, device):
     b.record()
     torch.cuda.synchronize()
     ms = a.elapsed_time(b) / 20
-    byts = sum(hpsi_bytes(sp.nc, mc.nc_of(N - 2, M), sp.P).values())
+    direct = sp.apply_h_profile(x, out, reps=1)[1] == 0.0
+    byts = direct_bytes(sp.nc) if direct else sum(hpsi_bytes(sp.nc, mc.nc_of(N - 2, M), sp.P).values())
     sp.ground(x.clone(), 100)                    # warm-up: the space keeps its Krylov basis
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -366,7 +390,8 @@ def run_large(mc, torch, device):
     occ = r1.diagonal().real.cpu().numpy()
     sp.close()
     return {"workload": "Lieb-Liniger N=20 M=10 g=10 (nc=10015005)", "hpsi_ms": ms,
-            "hpsi_per_s": 1e3 / ms, "hpsi_gbs": byts / (ms * 1e-3) / 1e9,
+            "hpsi_per_s": 1e3 / ms, "hpsi_form": "direct" if direct else "two kernels",
+            "hpsi_gbs": byts / (ms * 1e-3) / 1e9,
             "lanczos_iterations": it, "E0": E0, "lanczos_seconds": t_lz,
             "rho1_ms": 1e3 * t_r1, "rho2_ms": 1e3 * t_r2,
             "occupations": [round(float(o), 6) for o in occ]}
@@ -597,17 +622,40 @@ def run_mcpi(args):
         a, b = sp.apply_h_profile(X[k % ROTATE], out, reps=1)
         k1 += a / (2 * ROTATE)
         k2 += b / (2 * ROTATE)
-    names = ["pair_annihilate", "pair_create"]
-    times = {"pair_annihilate": k1, "pair_create": k2}
-    dom = max(names, key=lambda n: times[n])
-    byts = hpsi_bytes(nc, nc2, P)
     peak, peak_kind = measured_peak()
-    achieved = byts[dom] / (times[dom] * 1e-3) / 1e9
+    launches_per_step = 1 if k2 == 0.0 else 2
+    if k2 == 0.0:
+        # the direct kernel (the default form for these real momentum blocks)
+        dom, t_dom, b_dom = "hpsi_direct", k1, direct_bytes(nc)
+        kernel_ms = {dom: k1}
+        gathers = direct_gathers(M, nc2)
+        extra = {"irreducible_bytes": 32 * nc, "terms_per_launch": hpsi_terms(M, nc2),
+                 "psi_gathers_per_launch": gathers,
+                 "l2_gather_tbs": 16 * gathers / (k1 * 1e-3) / 1e12}
+    else:
+        names = ["pair_annihilate", "pair_create"]
+        times = {"pair_annihilate": k1, "pair_create": k2}
+        dom = max(names, key=lambda n: times[n])
+        byts = hpsi_bytes(nc, nc2, P)
+        t_dom, b_dom, kernel_ms = times[dom], byts[dom], times
+        extra = {"irreducible_bytes": 32 * nc}
+    achieved = b_dom / (t_dom * 1e-3) / 1e9
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_source": peak_kind,
-                "traffic": ncu_traffic(dom), "algorithmic_bytes": byts[dom],
-                "kernel_ms": {n: times[n] for n in names},
-                "hpsi_achieved_gbs": (byts["pair_annihilate"] + byts["pair_create"]) / (ms / args.steps * 1e-3) / 1e9}
+                "traffic": ncu_traffic(dom), "algorithmic_bytes": b_dom, **extra, "kernel_ms": kernel_ms}
+    # the two pair kernels on the same states, for comparison (MCPI_OPT_DIRECT_HPSI = 0)
+    if k2 == 0.0:
+        sp.set_option(mc.OPT_DIRECT_HPSI, 0)
+        for w in range(3):
+            sp.apply_h(X[w % ROTATE], out)
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record()
+        for k in range(args.steps):
+            sp.apply_h(X[k % ROTATE], out)
+        t1.record()
+        torch.cuda.synchronize()
+        roofline["two_kernel_form_ms"] = t0.elapsed_time(t1) / args.steps
+        sp.set_option(mc.OPT_DIRECT_HPSI, 2)
 
     # ---- e2e through the C ABI with HOST buffers (mcpi_apply_h_host) ----
     # every step copies its state in from pinned host memory and its result
@@ -692,7 +740,7 @@ def run_mcpi(args):
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
                 "config": config(), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
-                "gpu_launches": 2 * args.steps, "clocks": clk, "lanczos": lanczos, "sharded": sharded,
+                "gpu_launches": launches_per_step * args.steps, "clocks": clk, "lanczos": lanczos, "sharded": sharded,
                 "adjoint": adjoint, "batched": batched, "large": large, "general": general}
         print(json.dumps(line), flush=True)
     sp.close()

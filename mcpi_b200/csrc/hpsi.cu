@@ -997,18 +997,22 @@ __global__ void __launch_bounds__(kTC, 4) k_pair_create_smem(Space sp, SpaceTabl
 // for b != a the orbitals q, l differ from k, s and one of two orders holds,
 // q < k <= s < l or k < q <= l < s. The prefix counts of v - a + b then move
 // by +1 on [q, k) and -1 on [s, l) (or -1 on [k, q) and +1 on [l, s)); with
-// per-row tables Dp[t] = sum_{i<t} W_i(P_i + 1) - W_i(P_i) and Dm (the same
-// with P_i - 1) the target index splits into a part of a and a part of b,
-//   q < k:  (base - Dp[k] + Dm[s]) + (Dp[q] - Dm[l])
-//   q > k:  (base + Dm[k] - Dp[s]) + (Dp[l] - Dm[q]),
-// formed once per block, so a term costs one addition for its index.
-// c_b(v - a) = sqrt((v_q+1)(v_l+1)) (sqrt((v_q+1)(v_q+2)) for q = l)
-// depends on v alone; the diagonal term b = a reads psi[v] with c_a(v)^2.
-// The gathers of R pairs of a block are issued together. REAL: the block
-// values are real (any real translation-invariant interaction), so a term is
-// a real coefficient times a complex gather -- two multiply-adds instead of
-// four, the same values. SMEM_D: the tables Dp, Dm sit in shared-memory
-// columns of their thread instead of registers.
+// per-row tables F[t] = sum_{i<t} W_i(P_i + 1) - W_i(P_i) and G (the same
+// with P_i - 1) the target index splits into a part of a and a part of b:
+// with YA(p) = F[q] - G[l], YB(p) = F[l] - G[q] for a pair p = (q, l),
+//   q < k:  (base - YA(a)) + YA(b)
+//   q > k:  (base - YB(a)) + YB(b),
+// two numbers per pair, formed once per block, so a term costs one addition
+// for its index. c_b(v - a) = sqrt((v_q+1)(v_l+1)) (sqrt((v_q+1)(v_q+2)) for
+// q = l) depends on v alone; the diagonal term b = a reads psi[v] with
+// c_a(v)^2. Square-root products come from a table sqrt(x) sqrt(y) in shared
+// memory; c_a(v) = 0 tells that a is not in v. The gathers of R creation
+// pairs of a block are issued together. REAL: the block values are real (any
+// real translation-invariant interaction), so a term is a real coefficient
+// times a complex gather -- two multiply-adds instead of four, the same
+// values. SMEM_D: the tables F, G sit in shared-memory columns of their
+// thread instead of registers. The kernel is bound by the SM's L1 data pipe
+// (the gathers and the table reads), not by HBM.
 // ---------------------------------------------------------------------------
 template <int M, bool REAL, int R, bool SMEM_D>
 __global__ void __launch_bounds__(kTC, 3)
@@ -1148,17 +1152,20 @@ __global__ void __launch_bounds__(kTC, 3)
     out[i - row0] = acc;
 }
 
-template <int M, bool REAL, int R, bool SMEM_D>
+template <int M, bool REAL>
 cudaError_t launch_direct(const Space &sp, const SpaceTables &tb, const MomBlocks<M> &hp, const double2 *hdiag,
                           const double2 *psi, double2 *out, cudaStream_t st, uint32_t row0, uint32_t row1)
 {
+    // two creation pairs' gathers in flight, the index tables in shared-memory
+    // columns (the fastest of the forms measured at N=16 and N=20, M=10)
+    constexpr int R = 2;
+    constexpr bool SMEM_D = true;
     const int ws = sp.wstride;
     const size_t smem = sizeof(double2) * M + sizeof(double) * ws * ws + sizeof(uint32_t) * (M - 1) * ws +
                         (SMEM_D ? 2 * sizeof(uint32_t) * M * kTC : 0);
     if (smem > 48 * 1024) {
-        const cudaError_t e =
-            cudaFuncSetAttribute(k_hpsi_direct<M, REAL, R, SMEM_D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem);
+        const cudaError_t e = cudaFuncSetAttribute(k_hpsi_direct<M, REAL, R, SMEM_D>,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
     const unsigned grid = (row1 - row0 + kTC - 1) / kTC;
@@ -1177,15 +1184,8 @@ cudaError_t direct_apply_m(const Space &sp, const SpaceTables &tb, const PairOp 
         hp.v[x] = op.hblk_host[x];
         real = real && hp.v[x].y == 0.0;
     }
-    const int form = op.direct;   // probe forms (3..6); 1 and 2 take the default
-    if (!real) {
-        if (form == 4) return launch_direct<M, false, 2, true>(sp, tb, hp, op.hdiag, psi, out, st, row0, row1);
-        return launch_direct<M, false, 1, true>(sp, tb, hp, op.hdiag, psi, out, st, row0, row1);
-    }
-    if (form == 3) return launch_direct<M, true, 1, true>(sp, tb, hp, op.hdiag, psi, out, st, row0, row1);
-    if (form == 5) return launch_direct<M, true, 1, false>(sp, tb, hp, op.hdiag, psi, out, st, row0, row1);
-    if (form == 6) return launch_direct<M, true, 2, false>(sp, tb, hp, op.hdiag, psi, out, st, row0, row1);
-    return launch_direct<M, true, 2, true>(sp, tb, hp, op.hdiag, psi, out, st, row0, row1);
+    if (real) return launch_direct<M, true>(sp, tb, hp, op.hdiag, psi, out, st, row0, row1);
+    return launch_direct<M, false>(sp, tb, hp, op.hdiag, psi, out, st, row0, row1);
 }
 
 }  // namespace
@@ -1204,14 +1204,8 @@ static int mom_count(int M)
 int hpsi_form(const Space &sp, const PairOp &op)
 {
     if (sp.N < 2 || sp.M < 2 || !op.hblk_host || op.nhblk != mom_count(sp.M)) return kFormTwo;
-    if (op.direct && sp.N < 64 && op.create_form == 0) {
-        bool take = op.direct != 2;
-        if (!take && sp.M <= kDirectAutoMaxM) {   // default: real blocks of up to kDirectAutoMaxM orbitals
-            take = true;
-            for (int x = 0; x < op.nhblk && take; ++x) take = op.hblk_host[x].y == 0.0;
-        }
-        if (take) return kFormDirect;
-    }
+    if (op.direct && sp.N < 64 && op.create_form == 0 && (op.direct != 2 || sp.M <= kDirectAutoMaxM))
+        return kFormDirect;
     if (op.fused.order && op.create_form == 0) return kFormFused;
     return kFormTwo;
 }

@@ -60,7 +60,7 @@ struct PairOp {
     // fused launch plan of the space (order == nullptr: two kernels)
     FusedPlan fused;
     // direct form: momentum-block integrals applied row by row with no
-    // intermediate (0 off, 1 on, 2 on for real blocks and M <= kDirectAutoMaxM)
+    // intermediate (0 off, 1 on, 2 on for M <= kDirectAutoMaxM)
     int direct;
 };
 
