@@ -166,12 +166,15 @@ def measured_peak():
 
 
 def ncu_traffic(kernel):
-    """DRAM bytes per launch of `kernel` from the committed ncu summary, or None."""
-    p = os.path.join(ROOT, "profiles", "hpsi_lieb_n16_m10.md")
-    if not os.path.exists(p):
-        return None
-    m = re.search(rf"^traffic_bytes_per_launch\s+{kernel}\s+([0-9.eE+]+)", open(p).read(), re.M)
-    return float(m.group(1)) if m else None
+    """DRAM bytes per launch of `kernel` from the committed ncu summaries, or None."""
+    for name in ("hpsi_direct_lieb_n16_m10.md", "hpsi_lieb_n16_m10.md"):
+        p = os.path.join(ROOT, "profiles", name)
+        if not os.path.exists(p):
+            continue
+        m = re.search(rf"^traffic_bytes_per_launch\s+{kernel}\s+([0-9.eE+]+)", open(p).read(), re.M)
+        if m:
+            return float(m.group(1))
+    return None
 
 
 def hpsi_bytes(nc, nc2, P):
