@@ -66,7 +66,7 @@ struct PairOp {
 
 // The form a whole-vector H.psi (both stages, all rows) takes with op.
 enum { kFormTwo = 0, kFormFused = 1, kFormDirect = 2 };
-constexpr int kDirectAutoMaxM = 10;
+constexpr int kDirectAutoMaxM = 11;
 int hpsi_form(const Space &sp, const PairOp &op);
 constexpr int kGemmMaxP = 78;   // M <= 12: Ht (zero-padded to a multiple of 8 rows) fits shared memory
 

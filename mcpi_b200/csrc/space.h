@@ -70,7 +70,7 @@ struct mcpi_space_s {
     int create_form = 0;            // pair-creation kernel form (MCPI_OPT_CREATE_FORM)
     // fused H.psi (MCPI_OPT_FUSED_*): schedule built once per space by ensure_fused
     bool fused_on = false;
-    int direct_on = 2;               // MCPI_OPT_DIRECT_HPSI (default: on for M <= 10)
+    int direct_on = 2;               // MCPI_OPT_DIRECT_HPSI (default: on for M <= 11)
     int fused_lead = 128;
     bool fz_ready = false;
     mcpi::FusedPlan fz{};

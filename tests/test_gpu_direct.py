@@ -74,7 +74,7 @@ def test_direct_against_two_kernels(N, M):
     sp.close()
 
 
-def test_direct_is_the_default_up_to_ten_orbitals():
+def test_direct_is_the_default_up_to_eleven_orbitals():
     for M, kind in ((7, "lieb"), (10, "lieb"), (11, "lieb"), (13, "lieb"), (8, "complex"), (12, "complex")):
         N = 6
         Ho, Hint = mc.lieb_integrals(M, 1.0) if kind == "lieb" else complex_momentum_integrals(M, 2)
@@ -82,7 +82,7 @@ def test_direct_is_the_default_up_to_ten_orbitals():
         sp.set_integrals(Ho, Hint)
         x = _state(sp.nc, M)
         one = sp.apply_h_profile(x, reps=1)[1] == 0.0
-        assert one == (M <= 10), (M, kind)
+        assert one == (M <= 11), (M, kind)
         sp.close()
 
 

@@ -63,18 +63,13 @@ def test_sharded_lanczos_nccl_one_rank():
         dist.destroy_process_group()
 
 
-def test_shard_primitives_three_virtual_ranks():
-    # three ranks with uneven row blocks emulated in one process on one GPU: each
-    # rank's shard of every step runs in the library's kernels (mcpi_shard_*,
-    # mcpi_apply_h_rows on the gathered vector), and the all-reduce is the sum of
-    # the ranks' device scalars -- the recurrence must match mcpi_lanczos
+def _virtual_ranks(sp, C0, lm, W):
+    """W ranks with uneven row blocks emulated in one process on one GPU: each
+    rank's shard of every step runs in the library's kernels (mcpi_shard_*,
+    mcpi_apply_h_rows on the gathered vector), and the all-reduce is the sum of
+    the ranks' device scalars. Returns (iterations, alpha, beta) on the host."""
     from mcpi_b200.distributed import DeviceShardOps, row_block
-    N, M, lm, W = 10, 8, 60, 3
-    sp = mc.FockSpace(N, M)
-    sp.set_integrals(*mc.lieb_integrals(M, 4.0))
     nc = sp.nc
-    assert nc % W != 0
-    C0 = torch.from_numpy(mc.random_problem(N, M, 103)[0]).cuda()
     blocks = [row_block(nc, W, r) for r in range(W)]
     dev = torch.device("cuda")
     ops = [DeviceShardOps(b - a, lm, dev) for a, b in blocks]
@@ -120,10 +115,31 @@ def test_shard_primitives_three_virtual_ranks():
         for r in range(W):
             ops[r].update(V[r], i + 2, R[r], V[r][i + 1], alpha[r][i + 1:i + 2], coef[r], norm2[r], done)
         allsum(norm2, slice(0, 1))
-    it1, alpha1, beta1, _ = sp.lanczos(C0, lm)
-    assert int(iters[0]) == it1 == lm
-    a = alpha[0].cpu().numpy()
+    out = int(iters[0]), alpha[0].cpu().numpy(), beta.cpu().numpy()
+    del V, R, full
+    return out
+
+
+@pytest.mark.parametrize("N,M,lm,W,g,direct", [(10, 8, 60, 3, 4.0, 2), (20, 11, 12, 4, 1.0, 2),
+                                                (20, 11, 12, 4, 1.0, 0)])
+def test_shard_primitives_virtual_ranks(N, M, lm, W, g, direct):
+    # uneven row blocks; the direct H.psi form on each rank's rows, or (direct
+    # = 0) the two pair kernels with kernel 1 over each block's E columns; N=20,
+    # M=11 (nc = 30,045,015) is beyond the reference's int32 maps. The
+    # recurrence must match mcpi_lanczos on the whole space.
+    sp = mc.FockSpace(N, M)
+    sp.set_option(mc.OPT_DIRECT_HPSI, direct)
+    sp.set_integrals(*mc.lieb_integrals(M, g))
+    assert sp.nc % W != 0
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(103)
+    C0 = torch.randn(sp.nc, dtype=torch.complex128, device="cuda", generator=gen)
+    C0 /= torch.linalg.vector_norm(C0)
+    it, a, b = _virtual_ranks(sp, C0, lm, W)
+    it1, alpha1, beta1, lvec = sp.lanczos(C0, lm)
+    del lvec
+    assert it == it1 == lm
     scale = np.abs(alpha1).max()
     assert np.abs(a - alpha1).max() <= 1e-10 * scale
-    assert np.abs(beta.cpu().numpy()[: lm - 1] - beta1[: lm - 1]).max() <= 1e-10 * scale
+    assert np.abs(b[: lm - 1] - beta1[: lm - 1]).max() <= 1e-10 * scale
     sp.close()
