@@ -6,8 +6,10 @@
 // member keeps the reference's recurrence (full classical Gram-Schmidt
 // reorthogonalisation, breakdown at beta_i / max beta < 1e-15) but each
 // stage is one launch over all members:
-//   * H.psi: one annihilation + one creation launch per orbital count M
-//     (hpsi.cu, k_batch_*), blocks assigned from (member, block) work tables;
+//   * H.psi: per orbital count M one launch of the direct kernel (M <= 9,
+//     no intermediate) or one annihilation + one creation launch through the
+//     members' E (hpsi.cu, k_batch_*), blocks assigned from (member, block)
+//     work tables;
 //   * vector stages: blocks assigned from (member, 2048-row tile) work tables,
 //     per-member partial sums reduced in a fixed order by one block per member;
 //   * a member whose Lanczos broke down sets its flag and every later block of
@@ -333,8 +335,11 @@ struct mcpi_batch_s {
         int2 *w1, *w2;     // member-major work tables
         int2 *w1i, *w2i;   // the same blocks interleaved across members (round robin)
         int n1, n2;
-        size_t sm1, sm2;
+        size_t sm1, sm2, sm3;
+        bool direct;       // the direct H.psi form (M <= kBatchDirectMaxM; the members hold no E)
+        int form;          // kBatch* as captured
     };
+    std::vector<char> mreal;   // member's block values are real
     std::vector<Group> groups;
     // batched H.psi schedule (the autotuner's second dimension): bit 0 = the
     // M groups run as concurrent graph branches (else one after another),
@@ -372,6 +377,7 @@ int mcpi_batch_create(int count, const int *N, const int *M, int lm, int device,
     b->device = device;
     b->spaces.assign(count, nullptr);
     b->ready.assign(count, 0);
+    b->mreal.assign(count, 1);
     auto cleanup = [&](int rc, const std::string &msg) {
         mcpi_batch_destroy(b);
         return bfail(rc, msg);
@@ -398,7 +404,8 @@ int mcpi_batch_create(int count, const int *N, const int *M, int lm, int device,
         off_r[m] = tot;
         tot += mcpi::up256(sizeof(double2) * nc);
         off_E[m] = tot;
-        tot += mcpi::up256(sizeof(double2) * (size_t)s->P * s->nc2);
+        if (M[m] > mcpi::kBatchDirectMaxM)   // the two-kernel form's intermediate
+            tot += mcpi::up256(sizeof(double2) * (size_t)s->P * s->nc2);
         off_S[m] = tot;
         tot += mcpi::up256(sizeof(double2) * nc);
         off_st[m] = tot;
@@ -431,7 +438,7 @@ int mcpi_batch_create(int count, const int *N, const int *M, int lm, int device,
         bm.nh = 0;
         bm.hdiag = nullptr;
         bm.lvec = z.V;
-        bm.E = reinterpret_cast<double2 *>(b->arena + off_E[m]);
+        bm.E = M[m] > mcpi::kBatchDirectMaxM ? reinterpret_cast<double2 *>(b->arena + off_E[m]) : nullptr;
         bm.r = z.r;
         bm.done = z.done;
         bm.occ = bm.occ2 = nullptr;
@@ -506,7 +513,10 @@ int mcpi_batch_create(int count, const int *N, const int *M, int lm, int device,
         (void)P;
         G.sm1 = mcpi::batch_smem(Ms[g], maxN, nh, 1);
         G.sm2 = mcpi::batch_smem(Ms[g], maxN, nh, 2);
-        e = mcpi::batch_prepare(Ms[g], G.sm1, G.sm2);
+        G.sm3 = mcpi::batch_smem(Ms[g], maxN, nh, 3);
+        G.direct = Ms[g] <= mcpi::kBatchDirectMaxM;
+        G.form = mcpi::kBatchTwo;
+        e = mcpi::batch_prepare(Ms[g], G.sm1, G.sm2, G.sm3);
         if (e != cudaSuccess) break;
         e = cudaMemcpy(G.w1, w1[g].data(), sizeof(int2) * w1[g].size(), cudaMemcpyHostToDevice);
         if (e == cudaSuccess) e = cudaMemcpy(G.w2, w2[g].data(), sizeof(int2) * w2[g].size(), cudaMemcpyHostToDevice);
@@ -545,6 +555,18 @@ int mcpi_batch_set_integrals(mcpi_batch b, int member, const double *h_Ho, const
     if (!s->fwd.hblk)
         return bfail(MCPI_ERR_ARG, "batched solves need integrals that conserve the total orbital index "
                                    "(momentum-conserving plane-wave integrals)");
+    bool real = true;
+    for (const double2 &h : s->fwd.hblk_h) real = real && h.y == 0.0;
+    b->mreal[member] = real;
+    if (b->exec && !real)   // a captured real-valued direct form no longer fits: capture again
+        for (const auto &G : b->groups)
+            if (G.M == s->M && G.form == mcpi::kBatchDirectReal) {
+                cudaStreamSynchronize(b->stream);
+                cudaGraphExecDestroy(b->exec);
+                cudaGraphDestroy(b->graph);
+                b->exec = nullptr;
+                b->graph = nullptr;
+            }
     BatchMember &bm = b->mem[member];
     bm.hblk = s->fwd.hblk;
     bm.nh = s->fwd.nhblk;
@@ -604,8 +626,8 @@ static cudaError_t enqueue_hpsi(mcpi_batch b, int vec, int sched)
     for (size_t g = 0; g < b->groups.size() && e == cudaSuccess; ++g) {
         const auto &G = b->groups[g];
         cudaStream_t s = branches && g > 0 ? b->side[g - 1] : st;
-        e = mcpi::launch_batch_apply_h(G.M, b->d_mem, inter ? G.w1i : G.w1, G.n1, G.sm1, inter ? G.w2i : G.w2, G.n2,
-                                       G.sm2, vec, s);
+        e = mcpi::launch_batch_apply_h(G.M, G.form, b->d_mem, inter ? G.w1i : G.w1, G.n1, G.sm1,
+                                       inter ? G.w2i : G.w2, G.n2, G.direct ? G.sm3 : G.sm2, vec, s);
         if (e == cudaSuccess && branches && g > 0) e = cudaEventRecord(b->ev_join[g - 1], s);
     }
     if (branches)
@@ -789,6 +811,12 @@ int mcpi_batch_run(mcpi_batch b, double *h_E0, int *h_iters)
     if (cudaSetDevice(b->device) != cudaSuccess) return bfail(MCPI_ERR_CUDA, "cudaSetDevice failed");
     cudaError_t e = cudaSuccess;
     if (!b->exec) {
+        for (auto &G : b->groups) {   // the H.psi form of each M group, fixed in the graph
+            bool real = true;
+            for (int m = 0; m < b->count; ++m)
+                if (b->spaces[m]->M == G.M) real = real && b->mreal[m];
+            G.form = !G.direct ? mcpi::kBatchTwo : real ? mcpi::kBatchDirectReal : mcpi::kBatchDirectComplex;
+        }
         e = b->tile == 0 ? autotune(b) : set_tile(b, b->tile);
         if (e == cudaSuccess && b->hsched < 0) e = autotune_hpsi(b);
         if (e != cudaSuccess) return bfail(MCPI_ERR_CUDA, std::string("batch schedule: ") + cudaGetErrorString(e));

@@ -1014,27 +1014,33 @@ __global__ void __launch_bounds__(kTC, 4) k_pair_create_smem(Space sp, SpaceTabl
 // thread instead of registers. The kernel is bound by the SM's L1 data pipe
 // (the gathers and the table reads), not by HBM.
 // ---------------------------------------------------------------------------
-template <int M, bool REAL, int R, bool SMEM_D>
-__global__ void __launch_bounds__(kTC, 3)
-    k_hpsi_direct(Space sp, SpaceTables tb, const __grid_constant__ MomBlocks<M> hp,
-                  const double2 *__restrict__ hdiag, const double2 *__restrict__ psi, double2 *__restrict__ out,
-                  uint32_t row0, uint32_t row1)
+// Shared memory of a direct block: hd[M] | sqrt(x) sqrt(y) [ws x ws] |
+// W [(M-1) x ws] | (SMEM_D) F, G [M x kTC] each.
+template <int M>
+constexpr size_t direct_smem(int ws, bool smem_d)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int ws = sp.wstride;
-    double2 *hd = reinterpret_cast<double2 *>(smem_raw);            // M
-    double *sqp = reinterpret_cast<double *>(hd + M);               // ws x ws: sqrt(x) sqrt(y)
-    uint32_t *W = reinterpret_cast<uint32_t *>(sqp + ws * ws);      // (M-1) x ws
-    uint32_t *FS = W + (M - 1) * ws, *GS = FS + M * kTC;            // SMEM_D: M x kTC each
-    for (int x = threadIdx.x; x < (M - 1) * ws; x += blockDim.x) W[x] = tb.W[x];
-    for (int x = threadIdx.x; x < ws * ws; x += blockDim.x) sqp[x] = tb.sq[x / ws] * tb.sq[x % ws];
-    if (threadIdx.x < M) hd[threadIdx.x] = hdiag[threadIdx.x];
-    __syncthreads();
+    return sizeof(double2) * M + sizeof(double) * ws * ws + sizeof(uint32_t) * (M - 1) * ws +
+           (smem_d ? 2 * sizeof(uint32_t) * M * kTC : 0);
+}
 
-    const uint32_t i = row0 + blockIdx.x * kTC + threadIdx.x;   // rows [row0, row1) -> out[i - row0]
-    if (i >= row1) return;
+template <int M>
+__device__ __forceinline__ void direct_tables(int ws, const uint32_t *gW, const double *gsq, const double2 *hdiag,
+                                              double2 *hd, double *sqp, uint32_t *W)
+{
+    for (int x = threadIdx.x; x < (M - 1) * ws; x += blockDim.x) W[x] = gW[x];
+    for (int x = threadIdx.x; x < ws * ws; x += blockDim.x) sqp[x] = gsq[x / ws] * gsq[x % ws];
+    if (threadIdx.x < M) hd[threadIdx.x] = hdiag[threadIdx.x];
+}
+
+// Row i of H.psi in the direct form into *dst; hv(x) is block value x.
+template <int M, bool REAL, int R, bool SMEM_D, class HV>
+__device__ __forceinline__ void direct_row(const Space &sp, const uint64_t *occ, int occ_bits, const uint32_t *W,
+                                           const double *sqp, const double2 *hd, uint32_t *FS, uint32_t *GS,
+                                           const HV &hv, const double2 *__restrict__ psi, double2 *dst, uint32_t i)
+{
+    const int ws = sp.wstride;
     int vv[M], P[M];
-    occupations<M>(tb.occ, tb.occ_bits, i, sp.N, sp.nc, W, ws, vv, P);
+    occupations<M>(occ, occ_bits, i, sp.N, sp.nc, W, ws, vv, P);
     const double2 x0 = __ldg(psi + i);
     double2 acc;
     {
@@ -1083,7 +1089,7 @@ __global__ void __launch_bounds__(kTC, 3)
         if (n == 1) {   // a single pair: only its diagonal term
             const int k = qlo, s = K - k;
             const double ca2 = k == s ? (double)(v(k) * (v(k) - 1)) : (double)(v(k) * v(s));
-            const double2 h = hp.v[off];
+            const double2 h = hv(off);
             cfma(acc, make_double2(h.x * ca2, h.y * ca2), x0);
             off += 1;
             continue;
@@ -1131,7 +1137,7 @@ __global__ void __launch_bounds__(kTC, 3)
 #pragma unroll
                         for (int c = 0; c < NB; ++c)
                             if (c < n) {
-                                const double2 h = hp.v[off + r * n + c];
+                                const double2 h = hv(off + r * n + c);
                                 const double w = c == r ? ca[rr] : cb[c];
                                 const double2 y = c == r ? x0 : gv[rr][c];
                                 if constexpr (REAL) {
@@ -1149,7 +1155,27 @@ __global__ void __launch_bounds__(kTC, 3)
             }
         off += n * n;
     }
-    out[i - row0] = acc;
+    *dst = acc;
+}
+
+template <int M, bool REAL, int R, bool SMEM_D>
+__global__ void __launch_bounds__(kTC, 3)
+    k_hpsi_direct(Space sp, SpaceTables tb, const __grid_constant__ MomBlocks<M> hp,
+                  const double2 *__restrict__ hdiag, const double2 *__restrict__ psi, double2 *__restrict__ out,
+                  uint32_t row0, uint32_t row1)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int ws = sp.wstride;
+    double2 *hd = reinterpret_cast<double2 *>(smem_raw);
+    double *sqp = reinterpret_cast<double *>(hd + M);
+    uint32_t *W = reinterpret_cast<uint32_t *>(sqp + ws * ws);
+    uint32_t *FS = W + (M - 1) * ws, *GS = FS + M * kTC;
+    direct_tables<M>(ws, tb.W, tb.sq, hdiag, hd, sqp, W);
+    __syncthreads();
+    const uint32_t i = row0 + blockIdx.x * kTC + threadIdx.x;   // rows [row0, row1) -> out[i - row0]
+    if (i >= row1) return;
+    direct_row<M, REAL, R, SMEM_D>(sp, tb.occ, tb.occ_bits, W, sqp, hd, FS, GS,
+                                   [&](int x) -> double2 { return hp.v[x]; }, psi, out + (i - row0), i);
 }
 
 template <int M, bool REAL>
@@ -1160,9 +1186,7 @@ cudaError_t launch_direct(const Space &sp, const SpaceTables &tb, const MomBlock
     // columns (the fastest of the forms measured at N=16 and N=20, M=10)
     constexpr int R = 2;
     constexpr bool SMEM_D = true;
-    const int ws = sp.wstride;
-    const size_t smem = sizeof(double2) * M + sizeof(double) * ws * ws + sizeof(uint32_t) * (M - 1) * ws +
-                        (SMEM_D ? 2 * sizeof(uint32_t) * M * kTC : 0);
+    const size_t smem = direct_smem<M>(sp.wstride, SMEM_D);
     if (smem > 48 * 1024) {
         const cudaError_t e = cudaFuncSetAttribute(k_hpsi_direct<M, REAL, R, SMEM_D>,
                                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -1490,22 +1514,58 @@ __global__ void __launch_bounds__(kTC, 4) k_batch_create(const BatchMember *__re
                         b.r, (uint32_t)w.y, 0u, b.sp.nc);
 }
 
+// The direct form for a batch: one launch, blocks of kTC rows of any member
+// (the creation work table), each block staging its member's block values in
+// shared memory (members differ, so they cannot be a kernel parameter).
+template <int M, bool REAL>
+__global__ void __launch_bounds__(kTC, 3) k_batch_direct(const BatchMember *__restrict__ mem,
+                                                      const int2 *__restrict__ work, int vec)
+{
+    const int2 w = work[blockIdx.x];
+    const BatchMember &b = mem[w.x];
+    if (*b.done) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int ws = b.sp.wstride;
+    double2 *hv = reinterpret_cast<double2 *>(smem_raw);            // mom_values<M>()
+    double2 *hd = hv + mom_values<M>();
+    double *sqp = reinterpret_cast<double *>(hd + M);
+    uint32_t *W = reinterpret_cast<uint32_t *>(sqp + ws * ws);
+    uint32_t *FS = W + (M - 1) * ws, *GS = FS + M * kTC;
+    for (int x = threadIdx.x; x < mom_values<M>(); x += blockDim.x) hv[x] = b.hblk[x];
+    direct_tables<M>(ws, b.W, b.sq, b.hdiag, hd, sqp, W);
+    __syncthreads();
+    const uint32_t i = (uint32_t)w.y * kTC + threadIdx.x;
+    if (i >= b.sp.nc) return;
+    direct_row<M, REAL, 2, true>(b.sp, b.occ, b.occ_bits, W, sqp, hd, FS, GS,
+                                 [&](int x) -> double2 { return hv[x]; }, b.lvec + (size_t)vec * b.sp.nc, b.r + i, i);
+}
+
 template <int M>
-cudaError_t batch_prepare_m(size_t smem1, size_t smem2)
+cudaError_t batch_prepare_m(size_t smem1, size_t smem2, size_t smem3)
 {
     cudaError_t e = cudaFuncSetAttribute(k_batch_annihilate<M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem1);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_batch_create<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_batch_direct<M, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem3);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_batch_direct<M, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem3);
     return e;
 }
 
 template <int M>
-cudaError_t batch_apply_m(const BatchMember *mem, const int2 *work1, int n1, size_t smem1,
+cudaError_t batch_apply_m(int form, const BatchMember *mem, const int2 *work1, int n1, size_t smem1,
                           const int2 *work2, int n2, size_t smem2, int vec, cudaStream_t st)
 {
-    if (n1) k_batch_annihilate<M><<<n1, kT2, smem1, st>>>(mem, work1, vec);
-    if (n2) k_batch_create<M><<<n2, kTC, smem2, st>>>(mem, work2, vec);
+    if (form == kBatchDirectReal) {
+        if (n2) k_batch_direct<M, true><<<n2, kTC, smem2, st>>>(mem, work2, vec);
+    } else if (form == kBatchDirectComplex) {
+        if (n2) k_batch_direct<M, false><<<n2, kTC, smem2, st>>>(mem, work2, vec);
+    } else {
+        if (n1) k_batch_annihilate<M><<<n1, kT2, smem1, st>>>(mem, work1, vec);
+        if (n2) k_batch_create<M><<<n2, kTC, smem2, st>>>(mem, work2, vec);
+    }
     return cudaGetLastError();
 }
 
@@ -1640,12 +1700,12 @@ cudaError_t apply_h_m(const Space &sp, const SpaceTables &tb, const PairOp &op, 
 
 }  // namespace
 
-cudaError_t launch_batch_apply_h(int M, const BatchMember *mem, const int2 *work1, int n1, size_t smem1,
+cudaError_t launch_batch_apply_h(int M, int form, const BatchMember *mem, const int2 *work1, int n1, size_t smem1,
                                  const int2 *work2, int n2, size_t smem2, int vec, cudaStream_t st)
 {
     switch (M) {
 #define MCPI_CASE(m) \
-    case m: return batch_apply_m<m>(mem, work1, n1, smem1, work2, n2, smem2, vec, st);
+    case m: return batch_apply_m<m>(form, mem, work1, n1, smem1, work2, n2, smem2, vec, st);
         MCPI_CASE(2) MCPI_CASE(3) MCPI_CASE(4) MCPI_CASE(5) MCPI_CASE(6) MCPI_CASE(7) MCPI_CASE(8)
         MCPI_CASE(9) MCPI_CASE(10) MCPI_CASE(11) MCPI_CASE(12) MCPI_CASE(13) MCPI_CASE(14)
         MCPI_CASE(15) MCPI_CASE(16)
@@ -1654,11 +1714,11 @@ cudaError_t launch_batch_apply_h(int M, const BatchMember *mem, const int2 *work
     }
 }
 
-cudaError_t batch_prepare(int M, size_t smem1, size_t smem2)
+cudaError_t batch_prepare(int M, size_t smem1, size_t smem2, size_t smem3)
 {
     switch (M) {
 #define MCPI_CASE(m) \
-    case m: return batch_prepare_m<m>(smem1, smem2);
+    case m: return batch_prepare_m<m>(smem1, smem2, smem3);
         MCPI_CASE(2) MCPI_CASE(3) MCPI_CASE(4) MCPI_CASE(5) MCPI_CASE(6) MCPI_CASE(7) MCPI_CASE(8)
         MCPI_CASE(9) MCPI_CASE(10) MCPI_CASE(11) MCPI_CASE(12) MCPI_CASE(13) MCPI_CASE(14)
         MCPI_CASE(15) MCPI_CASE(16)
@@ -1672,6 +1732,9 @@ size_t batch_smem(int M, int N, int nh, int stage)
     const int ws = N + 3;
     const size_t tab = sizeof(double) * ws + sizeof(uint32_t) * (M - 1) * ws;
     if (stage == 1) return sizeof(double2) * nh + tab;
+    if (stage == 3)   // the direct form: block values | hd | sqrt products | W | F, G
+        return sizeof(double2) * (nh + M) + sizeof(double) * ws * ws + sizeof(uint32_t) * (M - 1) * ws +
+               2 * sizeof(uint32_t) * M * kTC;
     return (sizeof(double) + 2 * sizeof(uint32_t)) * M * kTC + ((M * kTC + 15) & ~15) + sizeof(double2) * M +
            tab;
 }

@@ -52,3 +52,15 @@ def case_keys(golden, prefix):
             kind, N, M = k[len(prefix) + 1:].split("_")
             out.append((kind, int(N), int(M)))
     return sorted(out)
+
+
+def complex_momentum_integrals(M, seed):
+    """Random complex integrals that conserve momentum: Hint[k,s,q,l] = 0 unless
+    k + s = q + l, with the bosonic 8-fold symmetry; diagonal one-body part."""
+    import mcpi_b200 as mc
+    rng = np.random.default_rng(seed)
+    Ho = np.diag(rng.standard_normal(M)).astype(np.complex128)
+    H = mc.symmetrize_hint(rng.standard_normal(M ** 4) + 1j * rng.standard_normal(M ** 4), M)
+    l, q, s, k = np.indices((M, M, M, M))            # flat index k + s M + q M^2 + l M^3
+    H[(k + s != q + l).reshape(-1)] = 0.0
+    return Ho, H

@@ -7,6 +7,7 @@ import numpy as np
 import pytest
 
 import mcpi_b200 as mc
+from conftest import complex_momentum_integrals
 
 pytestmark = pytest.mark.gpu
 
@@ -93,6 +94,40 @@ def test_batch_schedules_agree():
         for k in range(len(members)):
             assert abs(E[k] - ref[k]) <= 1e-10 * max(1.0, abs(ref[k])), (tile, k, E[k], ref[k])
         b.close()
+
+
+def test_batch_hpsi_forms_against_single_solves():
+    # one batch mixing the direct H.psi form (M <= 9: real Lieb blocks, and
+    # complex momentum blocks) with the two pair kernels (M = 11, 12, 13):
+    # every member's E0 matches its own single-space solve
+    members = [(7, 9), (6, 8), (5, 12), (4, 13), (8, 11), (5, 8)]
+    ints = [mc.lieb_integrals(9, 1.5), complex_momentum_integrals(8, 5), mc.lieb_integrals(12, 3.0),
+            mc.lieb_integrals(13, 0.5), mc.lieb_integrals(11, 8.0), complex_momentum_integrals(8, 6)]
+    lm = 40
+    b = mc.Batch(members, lm)
+    starts = []
+    for k, ((N, M), (Ho, Hint)) in enumerate(zip(members, ints)):
+        b.set_integrals(k, Ho, Hint)
+        starts.append(_start(b.nc[k], 400 + k))
+        b.set_start(k, starts[k])
+    E, it = b.run()
+    for k, ((N, M), (Ho, Hint)) in enumerate(zip(members, ints)):
+        sp = mc.FockSpace(N, M)
+        sp.set_integrals(Ho, Hint)
+        Es, _, its = sp.ground(starts[k], lm)
+        assert it[k] == its, (k, it[k], its)
+        assert abs(E[k] - Es) <= 1e-10 * max(1.0, abs(Es)), (k, E[k], Es)
+        sp.close()
+    # a member's integrals turning complex after the capture: the batch captures again
+    b.set_integrals(0, *complex_momentum_integrals(9, 7))
+    E2, it2 = b.run()
+    sp = mc.FockSpace(7, 9)
+    sp.set_integrals(*complex_momentum_integrals(9, 7))
+    Es = sp.ground(starts[0], lm)[0]
+    assert abs(E2[0] - Es) <= 1e-10 * max(1.0, abs(Es))
+    assert np.array_equal(E2[1:], E[1:])
+    sp.close()
+    b.close()
 
 
 def test_batch_hpsi_schedules_agree():

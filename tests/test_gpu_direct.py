@@ -13,21 +13,10 @@ import pytest
 import torch
 
 import mcpi_b200 as mc
-from conftest import rel
+from conftest import complex_momentum_integrals, rel
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-12
-
-
-def complex_momentum_integrals(M, seed):
-    """Random complex integrals that conserve momentum: Hint[k,s,q,l] = 0 unless
-    k + s = q + l, with the 8-fold symmetry; diagonal one-body part."""
-    rng = np.random.default_rng(seed)
-    Ho = np.diag(rng.standard_normal(M)).astype(np.complex128)
-    H = mc.symmetrize_hint(rng.standard_normal(M ** 4) + 1j * rng.standard_normal(M ** 4), M)
-    l, q, s, k = np.indices((M, M, M, M))            # flat index k + s M + q M^2 + l M^3
-    H[(k + s != q + l).reshape(-1)] = 0.0
-    return Ho, H
 
 
 def _space(N, M, direct, Ho, Hint):
