@@ -68,6 +68,8 @@ def parse():
     p.add_argument("--no-adjoint", action="store_true")
     p.add_argument("--profile", choices=["batch", "lanczos", "density", "hpsi"], default=None,
                    help="run only this section (for profiler launch lists), print its timings")
+    p.add_argument("--particles", type=int, default=None,
+                   help="--profile density: particles of the Lieb-Liniger workload (default 16; M = 10)")
     return p.parse_args()
 
 
@@ -777,7 +779,8 @@ def run_profile(args):
         out = {"section": "batch", "seconds": dt, "schedule": b.schedule()[0]}
         b.close()
     elif args.profile == "density":
-        sp = mc.FockSpace(N_PART, M_ORB, device=0)
+        n_part = args.particles or N_PART
+        sp = mc.FockSpace(n_part, M_ORB, device=0)
         sp.set_integrals(*mc.lieb_integrals(M_ORB, G, L_RING))
         gen = torch.Generator(device=sp.torch_device)
         gen.manual_seed(1234)
@@ -785,7 +788,7 @@ def run_profile(args):
                 for _ in range(2))
         x /= torch.linalg.vector_norm(x)
         y /= torch.linalg.vector_norm(y)
-        out = {"section": "density", "workload": f"Lieb-Liniger N={N_PART} M={M_ORB} (nc={sp.nc})"}
+        out = {"section": "density", "workload": f"Lieb-Liniger N={n_part} M={M_ORB} (nc={sp.nc})"}
         for name, f in (("rho1", lambda: sp.rho1(x)), ("rho2", lambda: sp.rho2(x)),
                         ("trans_rho2", lambda: sp.trans_rho2(y, x))):
             for _ in range(args.warmup):
