@@ -338,6 +338,15 @@ struct mcpi_batch_s {
         size_t sm1, sm2, sm3;
         bool direct;       // the direct H.psi form (M <= kBatchDirectMaxM; the members hold no E)
         int form;          // kBatch* as captured
+        // the real-valued direct form: members in launches of up to
+        // batch_chunk_members(M), their block values a kernel parameter
+        struct Chunk {
+            int2 *w, *wi;   // (slot, block) work tables, member-major / interleaved
+            int n;
+            std::vector<int> members;
+            std::vector<unsigned char> vals;   // filled when the solve is captured
+        };
+        std::vector<Chunk> chunks;
     };
     std::vector<char> mreal;   // member's block values are real
     std::vector<Group> groups;
@@ -471,11 +480,40 @@ int mcpi_batch_create(int count, const int *N, const int *M, int lm, int device,
             for (int m = 0; m < count; ++m)
                 if (M[m] == Ms[g] && k < (b->spaces[m]->nc + rpb2 - 1) / rpb2) w2i[g].push_back(make_int2(m, (int)k));
     }
+    // chunks of the direct groups: (slot, block) tables
+    std::vector<std::vector<std::vector<int>>> cmem(Ms.size());
+    std::vector<std::vector<std::vector<int2>>> cw(Ms.size()), cwi(Ms.size());
+    for (size_t g = 0; g < Ms.size(); ++g) {
+        if (Ms[g] > mcpi::kBatchDirectMaxM) continue;
+        const int cap = mcpi::batch_chunk_members(Ms[g]);
+        for (int m = 0; m < count; ++m) {
+            if (M[m] != Ms[g]) continue;
+            if (cmem[g].empty() || (int)cmem[g].back().size() == cap) cmem[g].emplace_back();
+            cmem[g].back().push_back(m);
+        }
+        for (const auto &mm : cmem[g]) {
+            std::vector<int2> a, ai;
+            int64_t most = 0;
+            for (size_t sl = 0; sl < mm.size(); ++sl) {
+                const int64_t nb = (b->spaces[mm[sl]]->nc + rpb2 - 1) / rpb2;
+                for (int64_t k = 0; k < nb; ++k) a.push_back(make_int2((int)sl, (int)k));
+                most = std::max(most, nb);
+            }
+            for (int64_t k = 0; k < most; ++k)
+                for (size_t sl = 0; sl < mm.size(); ++sl)
+                    if (k < (b->spaces[mm[sl]]->nc + rpb2 - 1) / rpb2) ai.push_back(make_int2((int)sl, (int)k));
+            cw[g].push_back(a);
+            cwi[g].push_back(ai);
+        }
+    }
     size_t mbytes = mcpi::up256(sizeof(BatchLz) * count) + mcpi::up256(sizeof(BatchMember) * count) +
                     mcpi::up256(sizeof(int2) * vwork.size()) + mcpi::up256(sizeof(double) * count) +
                     mcpi::up256(sizeof(int) * count);
-    for (size_t g = 0; g < Ms.size(); ++g)
+    for (size_t g = 0; g < Ms.size(); ++g) {
         mbytes += 2 * (mcpi::up256(sizeof(int2) * w1[g].size()) + mcpi::up256(sizeof(int2) * w2[g].size()));
+        for (size_t c = 0; c < cw[g].size(); ++c)
+            mbytes += mcpi::up256(sizeof(int2) * cw[g][c].size()) + mcpi::up256(sizeof(int2) * cwi[g][c].size());
+    }
     if (cudaMalloc(&b->meta, mbytes) != cudaSuccess) return cleanup(MCPI_ERR_NOMEM, "metadata allocation failed");
     char *p = b->meta;
     auto take = [&](size_t bytes) {
@@ -522,6 +560,18 @@ int mcpi_batch_create(int count, const int *N, const int *M, int lm, int device,
         if (e == cudaSuccess) e = cudaMemcpy(G.w2, w2[g].data(), sizeof(int2) * w2[g].size(), cudaMemcpyHostToDevice);
         if (e == cudaSuccess) e = cudaMemcpy(G.w1i, w1i[g].data(), sizeof(int2) * w1i[g].size(), cudaMemcpyHostToDevice);
         if (e == cudaSuccess) e = cudaMemcpy(G.w2i, w2i[g].data(), sizeof(int2) * w2i[g].size(), cudaMemcpyHostToDevice);
+        for (size_t c = 0; c < cw[g].size() && e == cudaSuccess; ++c) {
+            mcpi_batch_s::Group::Chunk C;
+            C.w = reinterpret_cast<int2 *>(take(sizeof(int2) * cw[g][c].size()));
+            C.wi = reinterpret_cast<int2 *>(take(sizeof(int2) * cwi[g][c].size()));
+            C.n = (int)cw[g][c].size();
+            C.members = cmem[g][c];
+            C.vals.assign(mcpi::batch_vals_bytes(Ms[g]), 0);
+            e = cudaMemcpy(C.w, cw[g][c].data(), sizeof(int2) * cw[g][c].size(), cudaMemcpyHostToDevice);
+            if (e == cudaSuccess)
+                e = cudaMemcpy(C.wi, cwi[g][c].data(), sizeof(int2) * cwi[g][c].size(), cudaMemcpyHostToDevice);
+            G.chunks.push_back(std::move(C));
+        }
         b->groups.push_back(G);
     }
     // side streams and events for the concurrent H.psi schedule
@@ -558,9 +608,9 @@ int mcpi_batch_set_integrals(mcpi_batch b, int member, const double *h_Ho, const
     bool real = true;
     for (const double2 &h : s->fwd.hblk_h) real = real && h.y == 0.0;
     b->mreal[member] = real;
-    if (b->exec && !real)   // a captured real-valued direct form no longer fits: capture again
+    if (b->exec)   // the real-valued direct form carries the values in the graph: capture again
         for (const auto &G : b->groups)
-            if (G.M == s->M && G.form == mcpi::kBatchDirectReal) {
+            if (G.M == s->M && G.form == mcpi::kBatchDirectReal && b->exec) {
                 cudaStreamSynchronize(b->stream);
                 cudaGraphExecDestroy(b->exec);
                 cudaGraphDestroy(b->graph);
@@ -626,8 +676,13 @@ static cudaError_t enqueue_hpsi(mcpi_batch b, int vec, int sched)
     for (size_t g = 0; g < b->groups.size() && e == cudaSuccess; ++g) {
         const auto &G = b->groups[g];
         cudaStream_t s = branches && g > 0 ? b->side[g - 1] : st;
-        e = mcpi::launch_batch_apply_h(G.M, G.form, b->d_mem, inter ? G.w1i : G.w1, G.n1, G.sm1,
-                                       inter ? G.w2i : G.w2, G.n2, G.direct ? G.sm3 : G.sm2, vec, s);
+        if (G.form == mcpi::kBatchDirectReal)
+            for (size_t c = 0; c < G.chunks.size() && e == cudaSuccess; ++c)
+                e = mcpi::launch_batch_direct_vals(G.M, b->d_mem, inter ? G.chunks[c].wi : G.chunks[c].w,
+                                                   G.chunks[c].n, G.sm3, vec, G.chunks[c].vals.data(), s);
+        else
+            e = mcpi::launch_batch_apply_h(G.M, G.form, b->d_mem, inter ? G.w1i : G.w1, G.n1, G.sm1,
+                                           inter ? G.w2i : G.w2, G.n2, G.direct ? G.sm3 : G.sm2, vec, s);
         if (e == cudaSuccess && branches && g > 0) e = cudaEventRecord(b->ev_join[g - 1], s);
     }
     if (branches)
@@ -816,6 +871,11 @@ int mcpi_batch_run(mcpi_batch b, double *h_E0, int *h_iters)
             for (int m = 0; m < b->count; ++m)
                 if (b->spaces[m]->M == G.M) real = real && b->mreal[m];
             G.form = !G.direct ? mcpi::kBatchTwo : real ? mcpi::kBatchDirectReal : mcpi::kBatchDirectComplex;
+            if (G.form == mcpi::kBatchDirectReal)
+                for (auto &C : G.chunks)
+                    for (size_t sl = 0; sl < C.members.size(); ++sl)
+                        mcpi::batch_fill_vals(G.M, C.vals.data(), (int)sl, C.members[sl],
+                                              b->spaces[C.members[sl]]->fwd.hblk_h.data());
         }
         e = b->tile == 0 ? autotune(b) : set_tile(b, b->tile);
         if (e == cudaSuccess && b->hsched < 0) e = autotune_hpsi(b);

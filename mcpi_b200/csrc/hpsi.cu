@@ -1540,6 +1540,42 @@ __global__ void __launch_bounds__(kTC, 3) k_batch_direct(const BatchMember *__re
                                  [&](int x) -> double2 { return hv[x]; }, b.lvec + (size_t)vec * b.sp.nc, b.r + i, i);
 }
 
+// Real block values of up to CAP members of one M, passed as a kernel
+// parameter (at most 30 KB of the 32 KB a launch takes): every block reads its
+// member's values through the constant bank, as the single-space kernel does,
+// instead of from shared memory.
+template <int M>
+struct BatchVals {
+    static constexpr int NV = mom_values<M>();
+    static constexpr int CAP = (30 * 1024) / (8 * NV + 4) < 64 ? (30 * 1024) / (8 * NV + 4) : 64;
+    double v[CAP][NV];
+    int member[CAP];
+};
+
+template <int M>
+__global__ void __launch_bounds__(kTC, 3) k_batch_direct_p(const BatchMember *__restrict__ mem,
+                                                        const int2 *__restrict__ work, int vec,
+                                                        const __grid_constant__ BatchVals<M> bv)
+{
+    const int2 w = work[blockIdx.x];   // (slot in bv, block of the member's rows)
+    const int slot = w.x;
+    const BatchMember &b = mem[bv.member[slot]];
+    if (*b.done) return;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int ws = b.sp.wstride;
+    double2 *hd = reinterpret_cast<double2 *>(smem_raw);
+    double *sqp = reinterpret_cast<double *>(hd + M);
+    uint32_t *W = reinterpret_cast<uint32_t *>(sqp + ws * ws);
+    uint32_t *FS = W + (M - 1) * ws, *GS = FS + M * kTC;
+    direct_tables<M>(ws, b.W, b.sq, b.hdiag, hd, sqp, W);
+    __syncthreads();
+    const uint32_t i = (uint32_t)w.y * kTC + threadIdx.x;
+    if (i >= b.sp.nc) return;
+    direct_row<M, true, 2, true>(b.sp, b.occ, b.occ_bits, W, sqp, hd, FS, GS,
+                                 [&](int x) -> double2 { return make_double2(bv.v[slot][x], 0.0); },
+                                 b.lvec + (size_t)vec * b.sp.nc, b.r + i, i);
+}
+
 template <int M>
 cudaError_t batch_prepare_m(size_t smem1, size_t smem2, size_t smem3)
 {
@@ -1551,6 +1587,8 @@ cudaError_t batch_prepare_m(size_t smem1, size_t smem2, size_t smem3)
         e = cudaFuncSetAttribute(k_batch_direct<M, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem3);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_batch_direct<M, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem3);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_batch_direct_p<M>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem3);
     return e;
 }
 
@@ -1706,6 +1744,72 @@ cudaError_t launch_batch_apply_h(int M, int form, const BatchMember *mem, const 
     switch (M) {
 #define MCPI_CASE(m) \
     case m: return batch_apply_m<m>(form, mem, work1, n1, smem1, work2, n2, smem2, vec, st);
+        MCPI_CASE(2) MCPI_CASE(3) MCPI_CASE(4) MCPI_CASE(5) MCPI_CASE(6) MCPI_CASE(7) MCPI_CASE(8)
+        MCPI_CASE(9) MCPI_CASE(10) MCPI_CASE(11) MCPI_CASE(12) MCPI_CASE(13) MCPI_CASE(14)
+        MCPI_CASE(15) MCPI_CASE(16)
+#undef MCPI_CASE
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+int batch_chunk_members(int M)
+{
+    switch (M) {
+#define MCPI_CASE(m) \
+    case m: return BatchVals<m>::CAP;
+        MCPI_CASE(2) MCPI_CASE(3) MCPI_CASE(4) MCPI_CASE(5) MCPI_CASE(6) MCPI_CASE(7) MCPI_CASE(8)
+        MCPI_CASE(9) MCPI_CASE(10) MCPI_CASE(11) MCPI_CASE(12) MCPI_CASE(13) MCPI_CASE(14)
+        MCPI_CASE(15) MCPI_CASE(16)
+#undef MCPI_CASE
+    default: return 0;
+    }
+}
+
+size_t batch_vals_bytes(int M)
+{
+    switch (M) {
+#define MCPI_CASE(m) \
+    case m: return sizeof(BatchVals<m>);
+        MCPI_CASE(2) MCPI_CASE(3) MCPI_CASE(4) MCPI_CASE(5) MCPI_CASE(6) MCPI_CASE(7) MCPI_CASE(8)
+        MCPI_CASE(9) MCPI_CASE(10) MCPI_CASE(11) MCPI_CASE(12) MCPI_CASE(13) MCPI_CASE(14)
+        MCPI_CASE(15) MCPI_CASE(16)
+#undef MCPI_CASE
+    default: return 0;
+    }
+}
+
+namespace {
+template <int M>
+void fill_vals_m(void *vals, int slot, int member, const double2 *hblk_host)
+{
+    auto *bv = static_cast<BatchVals<M> *>(vals);
+    bv->member[slot] = member;
+    for (int x = 0; x < BatchVals<M>::NV; ++x) bv->v[slot][x] = hblk_host[x].x;
+}
+}  // namespace
+
+void batch_fill_vals(int M, void *vals, int slot, int member, const double2 *hblk_host)
+{
+    switch (M) {
+#define MCPI_CASE(m) \
+    case m: fill_vals_m<m>(vals, slot, member, hblk_host); break;
+        MCPI_CASE(2) MCPI_CASE(3) MCPI_CASE(4) MCPI_CASE(5) MCPI_CASE(6) MCPI_CASE(7) MCPI_CASE(8)
+        MCPI_CASE(9) MCPI_CASE(10) MCPI_CASE(11) MCPI_CASE(12) MCPI_CASE(13) MCPI_CASE(14)
+        MCPI_CASE(15) MCPI_CASE(16)
+#undef MCPI_CASE
+    default: break;
+    }
+}
+
+cudaError_t launch_batch_direct_vals(int M, const BatchMember *mem, const int2 *work, int n, size_t smem, int vec,
+                                     const void *vals, cudaStream_t st)
+{
+    if (n <= 0) return cudaSuccess;
+    switch (M) {
+#define MCPI_CASE(m) \
+    case m:                                                                                              \
+        k_batch_direct_p<m><<<n, kTC, smem, st>>>(mem, work, vec, *static_cast<const BatchVals<m> *>(vals)); \
+        return cudaGetLastError();
         MCPI_CASE(2) MCPI_CASE(3) MCPI_CASE(4) MCPI_CASE(5) MCPI_CASE(6) MCPI_CASE(7) MCPI_CASE(8)
         MCPI_CASE(9) MCPI_CASE(10) MCPI_CASE(11) MCPI_CASE(12) MCPI_CASE(13) MCPI_CASE(14)
         MCPI_CASE(15) MCPI_CASE(16)

@@ -148,16 +148,22 @@ struct BatchMember {
 // (members need E), or the direct kernel over work2's row blocks with smem2
 // = batch_smem(M, N, nh, 3) (real or complex block values).
 enum { kBatchTwo = 0, kBatchDirectReal = 1, kBatchDirectComplex = 2 };
-// Orbital counts up to which a batch takes the direct form. Its blocks read
-// their member's block values from shared memory (members differ), which costs
-// L1 bandwidth the single-space kernel saves with constant-bank operands: at
-// M = 11 the two pair kernels were faster in the 64-solve sweep (423 against
-// 476 ms over its 256 launches), at M = 9 the direct form (68 against 72 ms).
-constexpr int kBatchDirectMaxM = 9;
+// Orbital counts up to which a batch takes the direct form (the single-space
+// default's range).
+constexpr int kBatchDirectMaxM = 11;
 cudaError_t launch_batch_apply_h(int M, int form, const BatchMember *mem, const int2 *work1, int n1, size_t smem1,
                                  const int2 *work2, int n2, size_t smem2, int vec, cudaStream_t st);
 // stage 1 / 2: the annihilation / creation kernels; 3: the direct kernel
 size_t batch_smem(int M, int N, int nh, int stage);
+// The direct form with real block values passed as a kernel parameter: up to
+// batch_chunk_members(M) members per launch, their values in a host buffer of
+// batch_vals_bytes(M) bytes filled slot by slot with batch_fill_vals (real
+// parts of the member's momentum-block values); work lists (slot, block).
+int batch_chunk_members(int M);
+size_t batch_vals_bytes(int M);
+void batch_fill_vals(int M, void *vals, int slot, int member, const double2 *hblk_host);
+cudaError_t launch_batch_direct_vals(int M, const BatchMember *mem, const int2 *work, int n, size_t smem, int vec,
+                                     const void *vals, cudaStream_t st);
 // Sets the kernels' shared-memory limits (call outside stream capture).
 cudaError_t batch_prepare(int M, size_t smem1, size_t smem2, size_t smem3);
 // configurations per block of the batched kernels: stage 1 annihilation, 2 creation

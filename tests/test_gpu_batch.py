@@ -97,9 +97,10 @@ def test_batch_schedules_agree():
 
 
 def test_batch_hpsi_forms_against_single_solves():
-    # one batch mixing the direct H.psi form (M <= 9: real Lieb blocks, and
-    # complex momentum blocks) with the two pair kernels (M = 11, 12, 13):
-    # every member's E0 matches its own single-space solve
+    # one batch mixing the direct H.psi form (M <= 11: real Lieb blocks as a
+    # kernel parameter, complex momentum blocks from shared memory) with the
+    # two pair kernels (M = 12, 13): every member's E0 matches its own
+    # single-space solve
     members = [(7, 9), (6, 8), (5, 12), (4, 13), (8, 11), (5, 8)]
     ints = [mc.lieb_integrals(9, 1.5), complex_momentum_integrals(8, 5), mc.lieb_integrals(12, 3.0),
             mc.lieb_integrals(13, 0.5), mc.lieb_integrals(11, 8.0), complex_momentum_integrals(8, 6)]
