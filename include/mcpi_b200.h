@@ -102,7 +102,7 @@ MCPI_API int mcpi_space_sync(mcpi_space sp);
 #define MCPI_OPT_FUSED_LEAD 9
 /* MCPI_OPT_DIRECT_HPSI: apply momentum-block integrals row by row, gathering
  * every term straight from the state, with no P x NC(N-2,M) intermediate
- * (whole-vector calls with N < 64; row ranges keep the two kernels).
+ * (N < 64; whole vectors and row ranges alike).
  * 0 off, 1 on, 2 (default) on for M <= 11, where it is the faster form. */
 #define MCPI_OPT_DIRECT_HPSI 11
 MCPI_API int mcpi_space_set_option(mcpi_space sp, int option, int value);
