@@ -167,16 +167,21 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-def ncu_traffic(kernel):
-    """DRAM bytes per launch of `kernel` from the committed ncu summaries, or None."""
+def ncu_figure(key, kernel):
+    """A per-kernel figure (`key kernel value` line) from the committed ncu summaries, or None."""
     for name in ("hpsi_direct_lieb_n16_m10.md", "hpsi_lieb_n16_m10.md"):
         p = os.path.join(ROOT, "profiles", name)
         if not os.path.exists(p):
             continue
-        m = re.search(rf"^traffic_bytes_per_launch\s+{kernel}\s+([0-9.eE+]+)", open(p).read(), re.M)
+        m = re.search(rf"^{key}\s+{kernel}\s+([0-9.eE+]+)", open(p).read(), re.M)
         if m:
             return float(m.group(1))
     return None
+
+
+def ncu_traffic(kernel):
+    """DRAM bytes per launch of `kernel` from the committed ncu summaries, or None."""
+    return ncu_figure("traffic_bytes_per_launch", kernel)
 
 
 def hpsi_bytes(nc, nc2, P):
@@ -636,7 +641,12 @@ def run_mcpi(args):
         gathers = direct_gathers(M, nc2)
         extra = {"irreducible_bytes": 32 * nc, "terms_per_launch": hpsi_terms(M, nc2),
                  "psi_gathers_per_launch": gathers,
-                 "l2_gather_tbs": 16 * gathers / (k1 * 1e-3) / 1e12}
+                 "l2_gather_tbs": 16 * gathers / (k1 * 1e-3) / 1e12,
+                 # what bounds this kernel instead of HBM (ncu, one launch of the same workload)
+                 "binding": {"unit": "SM L1 data pipe (psi gathers + per-row index tables), then issue",
+                             "l1_data_pipe_pct": ncu_figure("l1_data_pipe_pct", dom),
+                             "issue_active_pct": ncu_figure("issue_active_pct", dom),
+                             "source": "profiles/hpsi_direct_lieb_n16_m10.md"}}
     else:
         names = ["pair_annihilate", "pair_create"]
         times = {"pair_annihilate": k1, "pair_create": k2}
