@@ -225,7 +225,12 @@ struct DmmaGram {
     // half the planes, so tiles of 64 configurations fit two stages -- with
     // sum planes and 32-configuration tiles it took 4.6 against 2.9 ms).
     static constexpr bool SUMS = !SAME;
-    static constexpr int NP = SAME ? 2 : 6;
+    // ASUM (one state, M <= 10): the gather warps also write the A-side sum
+    // plane Ar - Ai, so the product warps' FP64 adds -- on the pipe the DMMAs
+    // use -- are only the B-side sums; three planes of 64 configurations fit
+    // two stages in shared memory up to 64 padded rows
+    static constexpr bool ASUM = SAME && KP <= 64;
+    static constexpr int NP = SAME ? (ASUM ? 3 : 2) : 6;
     static constexpr int GM = SAME ? 64 : 32;        // configurations per tile
     static constexpr int LD = GM + 4;                // plane row stride (doubles)
     // gather warps: 8 for one state up to M = 10 (four threads per
@@ -333,6 +338,7 @@ __device__ __forceinline__ void dmma_gather(const Space &sp, const SpaceTables &
                 const double xr = c * x[k].x, xi = c * x[k].y;
                 pl[col * LD + ml] = xr;
                 pl[(KP + col) * LD + ml] = xi;
+                if constexpr (D::ASUM) pl[(2 * KP + col) * LD + ml] = xr - xi;
                 if constexpr (D::SUMS) {
                     const double yr = c * y[k].x, yi = c * y[k].y;
                     pl[(2 * KP + col) * LD + ml] = xr - xi;
@@ -427,7 +433,7 @@ __global__ void __launch_bounds__(DmmaGram<M, SAME>::THREADS, 1)
         }
         const double *Ar = planes + (size_t)st * D::NP * KP * LD;
         const double *Ai = Ar + KP * LD;
-        const double *As = Ar + 2 * KP * LD;                                      // SUMS only
+        const double *As = Ar + 2 * KP * LD;                                      // SUMS, ASUM
         const double *Br = SAME ? Ar : Ar + 3 * KP * LD;
         const double *Bi = SAME ? Ai : Ar + 4 * KP * LD;
         const double *Bs = Ar + 5 * KP * LD;                                      // SUMS only
@@ -446,7 +452,7 @@ __global__ void __launch_bounds__(DmmaGram<M, SAME>::THREADS, 1)
                     ar1 = Ar[r1];
                     ai0 = Ai[r0];
                     ai1 = Ai[r1];
-                    if constexpr (D::SUMS) {
+                    if constexpr (D::SUMS || D::ASUM) {
                         as0 = As[r0];
                         as1 = As[r1];
                     } else {
