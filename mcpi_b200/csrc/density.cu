@@ -250,7 +250,16 @@ struct DmmaGram {
         return n;
     }
     static constexpr int NT = ntiles();
-    static constexpr int TPW = (NT + kDmmaPW - 1) / kDmmaPW;   // tiles per product warp
+    static constexpr int TPW = (NT + kDmmaPW - 1) / kDmmaPW;   // most tiles of one product warp
+    // product warp w takes tiles [tstart(w), tstart(w) + tcount(w)): the tiles
+    // split as evenly as they go, so warps w and w + 4, which share an SM
+    // sub-partition's tensor core, hold nearly the same work (the transition
+    // form at M = 10: 28 tiles as 4,4,4,4,3,3,3,3 rather than seven warps of 4)
+    static constexpr __host__ __device__ int tcount(int w) { return NT / kDmmaPW + (w < NT % kDmmaPW ? 1 : 0); }
+    static constexpr __host__ __device__ int tstart(int w)
+    {
+        return w * (NT / kDmmaPW) + (w < NT % kDmmaPW ? w : NT % kDmmaPW);
+    }
     static constexpr size_t stage_bytes = sizeof(double) * NP * KP * LD;
     // planes, then the stage barriers, then the space's sqrt and binomial tables
     static size_t smem(int ws)
@@ -413,7 +422,7 @@ __global__ void __launch_bounds__(DmmaGram<M, SAME>::THREADS, 1)
         return;
     }
 
-    // product warps: tiles n = warp * TPW + x
+    // product warps: tiles n = tstart(warp) + x, x < tcount(warp)
     const int gq = lane >> 2, tq = lane & 3;
     double acc[D::TPW][3][4];
 #pragma unroll
@@ -423,8 +432,9 @@ __global__ void __launch_bounds__(DmmaGram<M, SAME>::THREADS, 1)
 #pragma unroll
             for (int z = 0; z < 4; ++z) acc[x][y][z] = 0.0;
     int ti[D::TPW], tj[D::TPW];
+    const int t0 = D::tstart(warp), tn = D::tcount(warp);
 #pragma unroll
-    for (int x = 0; x < D::TPW; ++x) dmma_tile<M, SAME>(warp * D::TPW + x, ti[x], tj[x]);
+    for (int x = 0; x < D::TPW; ++x) dmma_tile<M, SAME>(t0 + (x < tn ? x : 0), ti[x], tj[x]);
     for (uint32_t it = 0; it < ntb; ++it) {
         const int st = it % kDmmaStages;
         if (!mbar_wait(full + st, (it / kDmmaStages) & 1, limit)) {
@@ -444,7 +454,7 @@ __global__ void __launch_bounds__(DmmaGram<M, SAME>::THREADS, 1)
             double ar0 = 0, ar1 = 0, ai0 = 0, ai1 = 0, as0 = 0, as1 = 0;
 #pragma unroll
             for (int x = 0; x < D::TPW; ++x) {
-                if (warp * D::TPW + x >= D::NT) break;
+                if (x >= tn) break;
                 if (ti[x] != icur) {   // warp-uniform: reload A only for a new row group
                     icur = ti[x];
                     const int r0 = (16 * icur + gq) * LD + cm, r1 = r0 + 8 * LD;
@@ -473,7 +483,7 @@ __global__ void __launch_bounds__(DmmaGram<M, SAME>::THREADS, 1)
     double2 *out = partial + (size_t)blockIdx.x * K * K;
 #pragma unroll
     for (int x = 0; x < D::TPW; ++x) {
-        if (warp * D::TPW + x >= D::NT) break;
+        if (x >= tn) break;
 #pragma unroll
         for (int z = 0; z < 4; ++z) {
             const int a = 16 * ti[x] + gq + (z >= 2 ? 8 : 0), b = 8 * tj[x] + 2 * tq + (z & 1);
