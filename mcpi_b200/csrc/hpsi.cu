@@ -1011,8 +1011,11 @@ __global__ void __launch_bounds__(kTC, 4) k_pair_create_smem(Space sp, SpaceTabl
 // real translation-invariant interaction), so a term is a real coefficient
 // times a complex gather -- two multiply-adds instead of four, the same
 // values. SMEM_D: the tables F, G sit in shared-memory columns of their
-// thread instead of registers. The kernel is bound by the SM's L1 data pipe
-// (the gathers and the table reads), not by HBM.
+// thread instead of registers. The kernel is bound on the SM (L1 data pipe,
+// then instruction issue), not by HBM. The products of creation pairs that a
+// row does not hold run predicated with c_a = 0: skipping them by branches,
+// divergent or warp-uniform, measured slower, because the straight-line code
+// keeps the gathers of every block in flight.
 // ---------------------------------------------------------------------------
 // Shared memory of a direct block: hd[M] | sqrt(x) sqrt(y) [ws x ws] |
 // W [(M-1) x ws] | (SMEM_D) F, G [M x kTC] each.
