@@ -105,3 +105,17 @@ def test_direct_lanczos_agrees_with_two_kernels():
     scale = np.abs(a0).max()
     assert np.abs(a0 - a1).max() <= 1e-10 * scale and np.abs(b0 - b1).max() <= 1e-10 * scale
     assert abs(E0 - E1) <= 1e-10 * abs(E0)
+
+
+@pytest.mark.parametrize("N,direct_expected", [(63, True), (64, False)])
+def test_direct_form_particle_limit(orc, N, direct_expected):
+    # the direct form's square-root table takes (N + 3)^2 doubles of shared
+    # memory: from N = 64 on, whole-vector calls take the two pair kernels
+    M = 3
+    Ho, Hint = mc.lieb_integrals(M, 1.5)
+    C = mc.random_problem(N, M, 9)[0]
+    sp = _space(N, M, 1, Ho, Hint)
+    got = sp.apply_h(C).cpu().numpy()
+    assert rel(got, orc.apply_h(N, M, C, Ho, Hint, mode=2)) <= TOL
+    assert (sp.apply_h_profile(torch.from_numpy(C).cuda(), reps=1)[1] == 0.0) == direct_expected
+    sp.close()
