@@ -531,6 +531,7 @@ int mcpi_space_destroy(mcpi_space sp)
     cudaFree(sp->d_status);
     cudaFree(sp->d_occ);
     cudaFree(sp->d_occ2);
+    cudaFree(sp->d_occ1);
     cudaFree(sp->d_basis);
     cudaFree(sp->d_lzblk);
     cudaFree(sp->d_lzr);
@@ -568,7 +569,8 @@ int mcpi_space_set_option(mcpi_space sp, int option, int value)
             cudaStreamSynchronize(sp->stream);
             cudaFree(sp->d_occ);
             cudaFree(sp->d_occ2);
-            sp->d_occ = sp->d_occ2 = nullptr;
+            cudaFree(sp->d_occ1);
+            sp->d_occ = sp->d_occ2 = sp->d_occ1 = nullptr;
             sp->occ_bits = 0;
         }
         return MCPI_OK;
@@ -964,6 +966,20 @@ static int density(mcpi_space sp, int order, const void *phi, const void *psi, v
     DeviceGuard g(sp->device);
     int rc = ensure_gram(sp);
     if (rc) return rc;
+    // rho1 reads the packed occupations of the (N-1)-space, built on its first
+    // call with the bits of the space's other tables (none: the kernel decodes)
+    if (order == 1 && !sp->d_occ1 && sp->occ_bits && sp->nc1 > 0) {
+        if (cudaMalloc(&sp->d_occ1, sizeof(uint64_t) * (size_t)sp->nc1) == cudaSuccess) {
+            mcpi::Space s1 = sp->sp;
+            s1.N = sp->N - 1;
+            s1.nc = (uint32_t)sp->nc1;
+            CK(mcpi::launch_pack_occ(s1, mcpi::SpaceTables{sp->d_W, sp->d_sq}, sp->d_occ1, sp->occ_bits,
+                                     sp->stream));
+        } else {
+            (void)cudaGetLastError();
+            sp->d_occ1 = nullptr;
+        }
+    }
     CK(mcpi::launch_density(sp->sp, sp->tables(), order, (const double2 *)phi, (const double2 *)psi,
                             sp->d_gram, (double2 *)out, sp->stream, sp->d_status, sp->wait_cycles,
                             sp->test_stall));

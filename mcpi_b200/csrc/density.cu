@@ -548,7 +548,7 @@ __global__ void __launch_bounds__(kThreads) k_rho1(Space sp, SpaceTables tb, con
         const uint32_t h = tile * kTile1 + t;
         if (h < nh) {
             int u[M], Q[M];
-            decode<M>(h, sp.N - 1, nh, W, sp.wstride, u, Q);
+            occupations<M>(tb.occ1, tb.occ_bits, h, sp.N - 1, nh, W, sp.wstride, u, Q);
             uint32_t B0[M], B1[M];
             prefix_table<M>(Q, 0, W, sp.wstride, B0);
             prefix_table<M>(Q, 1, W, sp.wstride, B1);

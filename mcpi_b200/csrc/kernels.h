@@ -94,6 +94,7 @@ struct SpaceTables {
     const uint64_t *occ = nullptr;
     int occ_bits = 0;
     const uint64_t *occ2 = nullptr;   // the same for the (N-2)-particle space (occ_bits bits)
+    const uint64_t *occ1 = nullptr;   // the same for the (N-1)-particle space (rho1; built on first use)
 };
 // Bits per orbital of the packed occupation table of an N-particle space (0:
 // M orbitals do not fit in 64 bits).

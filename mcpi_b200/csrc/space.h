@@ -85,6 +85,7 @@ struct mcpi_space_s {
     size_t basis_cap = 0, lzblk_cap = 0, lzr_cap = 0;
     uint64_t *d_occ = nullptr;       // packed occupations of the space's rows (built by mcpi_set_integrals)
     uint64_t *d_occ2 = nullptr;      // the same for the (N-2)-particle space
+    uint64_t *d_occ1 = nullptr;      // the same for the (N-1)-particle space (first rho1 call)
     int occ_bits = 0;
-    mcpi::SpaceTables tables() const { return mcpi::SpaceTables{d_W, d_sq, d_occ, occ_bits, d_occ2}; }
+    mcpi::SpaceTables tables() const { return mcpi::SpaceTables{d_W, d_sq, d_occ, occ_bits, d_occ2, d_occ1}; }
 };
