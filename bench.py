@@ -723,6 +723,28 @@ def run_mcpi(args):
     barrier()
     sms = max_over_ranks(a0.elapsed_time(a1))
     e2e["one_state_per_call"] = {"value": world * ke / (sms / 1e3), "unit": UNIT}
+    # the host link's own bound: the same state-sized copies in and out at once
+    # on two streams with no H.psi (states per second = what e2e can reach)
+    s_in, s_out = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+    dy = torch.empty_like(dx)
+    torch.cuda.synchronize()
+    l0, l1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0.record()
+    s_in.wait_event(l0)
+    s_out.wait_event(l0)
+    for k in range(ke):
+        with torch.cuda.stream(s_in):
+            dx.copy_(hX[k % ROTATE], non_blocking=True)
+        with torch.cuda.stream(s_out):
+            hO[k % ROTATE].copy_(dy, non_blocking=True)
+    torch.cuda.current_stream(dev).wait_stream(s_in)
+    torch.cuda.current_stream(dev).wait_stream(s_out)
+    l1.record()
+    torch.cuda.synchronize()
+    lms = max_over_ranks(l0.elapsed_time(l1))
+    e2e["host_link_bound"] = {"value": world * ke / (lms / 1e3), "unit": UNIT,
+                              "gbs_each_way": 16 * nc * ke / (lms / 1e3) / 1e9,
+                              "what": "state-sized copies in and out at once, no H.psi"}
 
     # ---- Lanczos ground state of the same configuration ----
     lanczos = None
