@@ -356,9 +356,11 @@ def test_occupation_tables_and_decode_agree(orc, N, M, kind):
     sp = _space(N, M)
     sp.set_integrals(Ho, Hint)
     with_tables = sp.apply_h(C).cpu().numpy()
+    r1_tables = sp.rho1(C).cpu().numpy()         # (N-1)-space table, built by this first call
     sp.set_option(7, 1)               # MCPI_OPT_NO_OCC_TABLES
     sp.set_integrals(Ho, Hint)
     decoded = sp.apply_h(C).cpu().numpy()
     assert np.array_equal(with_tables, decoded)
+    assert np.array_equal(r1_tables, sp.rho1(C).cpu().numpy())
     assert rel(decoded, orc.apply_h(N, M, C, Ho, Hint, mode=2)) <= TOL
     sp.close()
